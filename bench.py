@@ -1,0 +1,445 @@
+#!/usr/bin/env python
+"""Sinkhorn WMD benchmark on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step = one full solve of one source document against the target
+set): V=100000 words, d=300, v_r=32 source words, N=5000 target documents with
+nnz ~ U[8,256] Zipf(1.1) ids, lambda=10, 15 iterations, seeded synthetic data
+standing in for the fastText/dbpedia inputs the reference uses.  Under torchrun
+each rank solves its own shard of 5000 documents (weak scaling, no data-path
+collective).
+
+Our arm prints one JSON line: ``value`` is WMD pairs/s with inputs resident in
+HBM (select + cost panel + fused Sinkhorn solve, CUDA events on the library's
+stream, L2 flushed between steps); ``e2e`` is the same metric through the
+drop-in C ABI call with pinned host buffers (H2D of r, the FP64 embeddings and
+the CSC matrix plus D2H of WMD inside every step); ``roofline`` covers the
+dominant kernel; ``cpu_baseline`` times the reference's own OpenMP solver on
+this host.  ``--impl reference`` times only the reference's CPU solver.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+PKG = "optimized-implementation-of-word-movers-distance_b200"
+
+METRIC = ("WMD pairs/s on 1 B200 at <=1e-4 rel err: plain vs batched+warm-start;"
+          " iters")
+UNIT = "pairs/s"
+WORKLOAD = dict(V=100_000, d=300, N=5000, v_r=32, nnz_lo=8, nnz_hi=256,
+                lam=10.0, max_iter=15)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="time budget of the CPU-baseline sample")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def make_problem(rank: int):
+    synth = importlib.import_module(PKG + ".synth")
+    W = WORKLOAD
+    cdf = synth.zipf_cdf(W["V"])
+    vecs = synth.embeddings(W["V"], W["d"], 1000, seed=0)
+    r = synth.source_doc(W["V"], W["v_r"], seed=1, cdf=cdf)
+    cp, ri, vv = synth.targets(W["V"], W["N"], W["nnz_lo"], W["nnz_hi"],
+                               seed=2 + rank, cdf=cdf)
+    return synth.Problem(vecs, r, cp, ri, vv, W["lam"], W["max_iter"])
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own solver (oracle/_ref) or, without it, the port.
+# ---------------------------------------------------------------------------
+def cpu_solver(p, cols: int):
+    """Returns (callable running one solve on the first `cols` documents,
+    kind, description)."""
+    import oracle
+    from oracle import oracle as O
+    N = min(cols, p.N)
+    cp = p.col_ptr[:N + 1]
+    nnz = int(cp[-1])
+    rows, vals = p.row_inds[:nnz], p.vals[:nnz]
+    vecs64 = p.vecs.astype(np.float64)
+    threads = host_cores()
+    if oracle.reference_available("fused"):
+        csr = oracle.csr_from_csc(p.V, N, cp, rows, vals)
+
+        def run():
+            return O.reference_sinkhorn(p.r, vecs64, *csr, N, p.lam,
+                                        p.max_iter, "fused", threads)
+        return run, "reference", N, threads
+
+    def run():
+        return oracle.sinkhorn(p.r, vecs64, cp, rows, vals, p.lam, p.max_iter,
+                               nthreads=threads)
+    return run, "port", N, threads
+
+
+def cpu_baseline(p, budget_s: float):
+    run, kind, N, threads = cpu_solver(p, p.N)
+    run()  # warm (page-in, thread pool)
+    calls, t0 = 0, time.perf_counter()
+    while True:
+        run()
+        calls += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or calls >= 50:
+            break
+    return {"value": calls * N / el, "unit": UNIT, "cores": threads,
+            "kind": kind,
+            "sample": f"{calls} full solves of the workload ({N} documents "
+                      f"each), {el:.1f} s, OpenMP threads={threads}"}
+
+
+def reference_arm(a, rank, world):
+    if rank != 0:
+        return 0
+    p = make_problem(0)
+    run_full, kind, _, threads = cpu_solver(p, p.N)
+    t0 = time.perf_counter()
+    run_full()
+    t_full = time.perf_counter() - t0
+    budget = 150.0
+    total = a.warmup + a.steps
+    cols = p.N
+    if total * t_full > budget:
+        # Shrink the per-step sample (leading documents of the same target
+        # set; per-document results are independent of the others).
+        cols = max(50, int(p.N * budget / (total * t_full)))
+    run, kind, N, threads = cpu_solver(p, cols)
+    for _ in range(a.warmup):
+        run()
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = a.steps * N / tot
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "single-source plain Sinkhorn WMD", **WORKLOAD,
+                   "docs_per_step": N},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": kind,
+                         "sample": f"{N} documents per step of the {p.N}-document "
+                                   f"workload, OpenMP threads={threads}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "50", "-i", str(device)],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        rows = []
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.flush()
+            self.f.seek(0)
+            for line in self.f.read().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        self.f.close()
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Our arm.
+# ---------------------------------------------------------------------------
+def ours(a, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1 and not dist.is_initialized():
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=dev)
+    wmd = importlib.import_module(PKG)
+    p = make_problem(rank)
+    W = WORKLOAD
+
+    eng = wmd.Engine(local)
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.set_timing(True)
+    r_dev = torch.from_numpy(p.r).to(dev)
+    out = torch.empty(p.N, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+
+    def step():
+        eng.query_device(r_dev.data_ptr(), W["v_r"], p.lam, p.max_iter,
+                         out.data_ptr())
+
+    # Correctness gate: the first solve is checked against the oracle on a
+    # sample of documents before anything is timed.
+    step()
+    eng.check()
+    import oracle
+    sub = 200
+    cp = p.col_ptr[:sub + 1]
+    ref = oracle.sinkhorn(p.r, p.vecs.astype(np.float64), cp,
+                          p.row_inds[:cp[-1]], p.vals[:cp[-1]], p.lam,
+                          p.max_iter)
+    got = out[:sub].cpu().numpy()
+    max_rel = float(np.max(np.abs(got - ref) / np.abs(ref)))
+    if not max_rel <= 1e-5:
+        raise SystemExit(f"bench: result check failed, max rel err {max_rel:.3e}")
+
+    sampler = ClockSampler(local)
+    t_settle = time.perf_counter()
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    # keep the GPU busy ~0.5 s before timing so the clock samples describe
+    # a loaded GPU
+    while time.perf_counter() - t_settle < 0.5:
+        step()
+        torch.cuda.synchronize(dev)
+    eng.check()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    stage = np.zeros((a.steps, 3))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    wall0 = time.perf_counter()
+    for k in range(a.steps):
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+        stage[k] = eng.stage_times()
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)  # evict L2 between steps (not timed)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop()
+    eng.check()
+    launches = eng.launch_count * a.steps
+    step_ms = np.array([s.elapsed_time(e) for s, e in ev])
+    tot_ms = float(step_ms.sum())
+    t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot_ms = float(t.item())
+    pairs = p.N * world * a.steps
+    value = pairs / (tot_ms / 1e3)
+
+    # Dominant kernel + roofline (per-launch averages over the timed steps).
+    sel_ms, cd_ms, sv_ms = stage.mean(axis=0)
+    nnz, vr, V, d, N = p.nnz, W["v_r"], W["V"], W["d"], p.N
+    it = W["max_iter"]
+    solve_bytes = it * (nnz * 8 + nnz * vr * 4 + 2 * N * vr * 4) + (
+        nnz * 8 + 2 * nnz * vr * 4 + 8 * N)
+    solve_flops = 4 * nnz * vr * (it + 1)
+    cdist_bytes = V * d * 4 + 2 * vr * V * 4
+    cdist_flops = 2 * vr * V * d
+    peak_hbm, peak_src = measured_peaks()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
+    dominant = "solve_kernel" if sv_ms >= cd_ms else "cdist_fp32_kernel"
+    if dominant == "solve_kernel":
+        ach = solve_bytes / (sv_ms * 1e-3) / 1e9
+        fl = solve_flops / (sv_ms * 1e-3) / 1e12
+    else:
+        ach = cdist_bytes / (cd_ms * 1e-3) / 1e9
+        fl = cdist_flops / (cd_ms * 1e-3) / 1e12
+    roofline = {
+        "bound": "hbm", "kernel": dominant, "achieved": ach, "peak": peak_hbm,
+        "unit": "GB/s", "frac": ach / peak_hbm,
+        "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+        "traffic": traffic_from_profiles(dominant),
+        "fp32_tflops": fl, "fp32_peak_tflops": fp32_peak,
+        "fp32_frac": fl / fp32_peak,
+        "stage_ms": {"select": sel_ms, "cdist": cd_ms, "solve": sv_ms},
+        "bytes_model": "per iteration nnz*8 + nnz*v_r*4 + 2*N*v_r*4, final "
+                       "nnz*8 + 2*nnz*v_r*4 + 8*N; cdist V*d*4 + 2*v_r*V*4",
+    }
+
+    # e2e through the drop-in C ABI with pinned host buffers.
+    vecs_h = torch.from_numpy(p.vecs.astype(np.float64)).pin_memory()
+    r_h = torch.from_numpy(p.r).pin_memory()
+    cp_h = torch.from_numpy(p.col_ptr.astype(np.int64)).pin_memory()
+    ri_h = torch.from_numpy(p.row_inds.astype(np.int64)).pin_memory()
+    vv_h = torch.from_numpy(p.vals).pin_memory()
+    args = (r_h.numpy(), vecs_h.numpy(), cp_h.numpy().view(np.uint64),
+            ri_h.numpy().view(np.uint64), vv_h.numpy())
+    h2d = sum(x.nbytes for x in args)
+    d2h = p.N * 8
+    for _ in range(2):
+        wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
+    e2e_t = []
+    for _ in range(a.e2e_steps):
+        t0 = time.perf_counter()
+        res = wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_tot = torch.tensor([sum(e2e_t)], dtype=torch.float64, device=dev)
+    # resident corpus: only r in, WMD out
+    eng2 = eng
+    res_t = []
+    for _ in range(a.e2e_steps):
+        t0 = time.perf_counter()
+        eng2.query(r_h.numpy(), p.lam, p.max_iter)
+        res_t.append(time.perf_counter() - t0)
+    res_tot = torch.tensor([sum(res_t)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+        dist.all_reduce(res_tot, op=dist.ReduceOp.MAX)
+    e2e_value = p.N * world * a.e2e_steps / float(e2e_tot.item())
+    res_value = p.N * world * a.e2e_steps / float(res_tot.item())
+    e2e_err = float(np.max(np.abs(res[:sub] - ref) / np.abs(ref)))
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(p, a.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": tot_ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "single-source plain Sinkhorn WMD "
+                                   "(FP32 cost panel + FP32 iterations, FP64 "
+                                   "final reduction)",
+                       **WORKLOAD, "nnz_per_rank": p.nnz,
+                       "docs_per_rank": p.N,
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"{world} independent document shards"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "api": "wmd_sinkhorn_fused_csc (drop-in, host buffers)",
+                    "resident_corpus_value": res_value,
+                    "resident_corpus_h2d_bytes_per_step": p.V * 8,
+                    "max_rel_err_vs_oracle": e2e_err},
+            "gpu_launches": launches,
+            "max_rel_err_vs_oracle": max_rel,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = args_()
+    if a.warmup < 3:
+        a.warmup = 3
+    rank, world, local = dist_env()
+    if a.impl == "reference":
+        return reference_arm(a, rank, world)
+    return ours(a, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,189 @@
+/*
+ * wmd_b200.h — C ABI of the B200 Sinkhorn Word Mover's Distance engine.
+ *
+ * Reference interface being replaced (IntelLabs/Optimized-Implementation-of-
+ * Word-Movers-Distance):
+ *
+ *   void sinkhorn_wmd(const double* r, const double* vecs, REAL* WMD,
+ *                     const REAL lamda, const int max_iter,
+ *                     const u64 data_vocab_size, const u64 num_docs,
+ *                     const u64 word2vec_word_embedding_size);
+ *       sinkhorn_wmd_fused.cpp:112-114, sinkhorn_wmd_nonfused.cpp:114-116
+ *
+ * whose target-document matrix is the global `puma_csr_double_t c_csr`
+ * (sinkhorn_wmd_fused.cpp:13, sinkhorn_wmd_nonfused.cpp:15).  The drop-in
+ * entry points below take the same arguments in the same order and meaning,
+ * plus that matrix as a trailing pointer.  All pointers of the drop-in calls
+ * are HOST pointers; the library copies to the GPU, solves there and copies
+ * WMD back before returning.
+ *
+ * Errors: where the reference asserts or exit(0)s (sinkhorn_wmd_fused.cpp:
+ * 131-153, 431-435, 474-478, 570-574), every call here returns a wmd_status
+ * and leaves a message for wmd_last_error().
+ *
+ * Threading: the drop-in calls are reentrant (each uses a per-thread default
+ * handle).  A wmd_handle must not be used by two host threads at once.
+ */
+#ifndef WMD_B200_H
+#define WMD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WMD_B200_ABI_VERSION 1
+
+typedef enum wmd_status {
+  WMD_OK = 0,
+  WMD_ERR_INVALID_ARG = 1,   /* bad pointer, size or option */
+  WMD_ERR_INVALID_INPUT = 2, /* data the reference driver rejects: r < 0,
+                                c value <= 0, word/doc index out of range,
+                                non-monotone column pointers */
+  WMD_ERR_OUT_OF_MEMORY = 3,
+  WMD_ERR_CUDA = 4,          /* CUDA runtime error; see wmd_last_error() */
+  WMD_ERR_NO_DEVICE = 5,
+  WMD_ERR_UNSUPPORTED = 6    /* option not available on this device/build */
+} wmd_status;
+
+/* Word-major target matrix; field-for-field the reference's
+ * puma_csr_double_t (common.h:38-46).  num_rows = vocabulary size V,
+ * num_cols = number of target documents N. */
+typedef struct wmd_csr_double_t {
+  uint64_t num_rows;
+  uint64_t num_cols;
+  uint64_t nnz;
+  uint64_t* row_ptr;  /* [num_rows + 1] */
+  uint64_t* col_inds; /* [nnz] document ids */
+  double* vals;       /* [nnz] normalised counts */
+} wmd_csr_double_t;
+
+/* Document-major target matrix; field-for-field the reference's
+ * puma_csc_double_t (common.h:49-57). */
+typedef struct wmd_csc_double_t {
+  uint64_t num_rows;
+  uint64_t num_cols;
+  uint64_t nnz;
+  uint64_t* col_ptr;  /* [num_cols + 1] */
+  uint64_t* row_inds; /* [nnz] word ids */
+  double* vals;       /* [nnz] */
+} wmd_csc_double_t;
+
+/* ---------------------------------------------------------------------------
+ * Drop-in solves (host buffers).
+ * ------------------------------------------------------------------------ */
+
+/* Replaces the fused sinkhorn_wmd (sinkhorn_wmd_fused.cpp:112-412).
+ * K = exp(lamda * M) exactly as sinkhorn_wmd_fused.cpp:217 computes it, so
+ * the usual regulariser lambda = 10 is passed as lamda = -10.  WMD receives
+ * num_docs values.  c_csr->num_rows must equal data_vocab_size and
+ * c_csr->num_cols must equal num_docs. */
+wmd_status wmd_sinkhorn_fused(const double* r, const double* vecs, double* WMD,
+                              double lamda, int max_iter,
+                              uint64_t data_vocab_size, uint64_t num_docs,
+                              uint64_t word2vec_word_embedding_size,
+                              const wmd_csr_double_t* c_csr);
+
+/* Replaces the nonfused sinkhorn_wmd (sinkhorn_wmd_nonfused.cpp:114-318).
+ * K = exp(-lamda * M) as sinkhorn_wmd_nonfused.cpp:172-173 computes it, so
+ * lambda = 10 is passed as lamda = +10.  Same math and results otherwise. */
+wmd_status wmd_sinkhorn_nonfused(const double* r, const double* vecs,
+                                 double* WMD, double lamda, int max_iter,
+                                 uint64_t data_vocab_size, uint64_t num_docs,
+                                 uint64_t word2vec_word_embedding_size,
+                                 const wmd_csr_double_t* c_csr);
+
+/* As wmd_sinkhorn_fused / wmd_sinkhorn_nonfused with the target matrix in
+ * the document-major layout the GPU iterates in (no transpose needed).
+ * Replaces the same reference functions. */
+wmd_status wmd_sinkhorn_fused_csc(const double* r, const double* vecs,
+                                  double* WMD, double lamda, int max_iter,
+                                  uint64_t data_vocab_size, uint64_t num_docs,
+                                  uint64_t word2vec_word_embedding_size,
+                                  const wmd_csc_double_t* c_csc);
+wmd_status wmd_sinkhorn_nonfused_csc(const double* r, const double* vecs,
+                                     double* WMD, double lamda, int max_iter,
+                                     uint64_t data_vocab_size,
+                                     uint64_t num_docs,
+                                     uint64_t word2vec_word_embedding_size,
+                                     const wmd_csc_double_t* c_csc);
+
+/* ---------------------------------------------------------------------------
+ * Handle API: embeddings and target set stay resident on the GPU across
+ * queries (the serving form of the same solve).  No reference counterpart:
+ * the reference re-reads its inputs on every run (sinkhorn_wmd_fused.cpp:
+ * 415-598).  lambda here is the positive regulariser: K = exp(-lambda * M).
+ * ------------------------------------------------------------------------ */
+
+typedef struct wmd_handle wmd_handle;
+
+/* Cost-matrix (cdist) precision. */
+typedef enum wmd_cdist_mode {
+  WMD_CDIST_FP32 = 0, /* FP32 CUDA-core GEMM form, near pairs recomputed */
+  WMD_CDIST_BF16 = 1, /* tcgen05 tensor cores, BF16 operands, FP32 accum */
+  WMD_CDIST_FP16 = 2  /* tcgen05 tensor cores, FP16 operands, FP32 accum */
+} wmd_cdist_mode;
+
+wmd_status wmd_create(wmd_handle** out, int device);
+wmd_status wmd_destroy(wmd_handle* h);
+
+/* Embeddings: V x d row-major.  `where` is 0 for host memory, 1 for device
+ * memory on the handle's GPU. */
+wmd_status wmd_set_embeddings_f64(wmd_handle* h, const double* vecs, uint64_t V,
+                                  uint64_t d, int where);
+wmd_status wmd_set_embeddings_f32(wmd_handle* h, const float* vecs, uint64_t V,
+                                  uint64_t d, int where);
+
+/* Target documents (host memory).  Validated on the GPU. */
+wmd_status wmd_set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c);
+wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* c);
+
+wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode);
+
+/* One source document as a dense host histogram r[V] (the reference's form,
+ * zeros skipped as sinkhorn_wmd_fused.cpp:45-63 does).  wmd_out: host, N. */
+wmd_status wmd_query_dense(wmd_handle* h, const double* r, double lambda,
+                           int max_iter, double* wmd_out);
+
+/* Device-resident variant: r_dev is a device pointer to V doubles, wmd_dev a
+ * device pointer to N doubles.  Runs asynchronously on the handle's stream
+ * (wmd_stream()); vr_cap bounds the number of non-zeros of r_dev (panels are
+ * sized for it; more non-zeros raise WMD_ERR_INVALID_INPUT at the next
+ * wmd_check()). */
+wmd_status wmd_query_dense_device(wmd_handle* h, const double* r_dev,
+                                  uint64_t vr_cap, double lambda, int max_iter,
+                                  double* wmd_dev);
+
+/* Synchronises the handle's stream and reports device-side validation
+ * failures of the calls issued since the previous check. */
+wmd_status wmd_check(wmd_handle* h);
+
+/* The handle's CUDA stream (a cudaStream_t), for event timing. */
+void* wmd_stream(wmd_handle* h);
+
+/* Number of kernels the last query launched. */
+int wmd_last_launch_count(wmd_handle* h);
+
+/* Stage timing.  While enabled, every query records CUDA events on the
+ * handle's stream around its three stages; wmd_stage_times waits for the
+ * last query and returns the select, cost-panel (cdist) and solve durations
+ * in milliseconds.  No reference counterpart (the reference times only the
+ * whole call, sinkhorn_wmd_fused.cpp:607-615). */
+wmd_status wmd_set_timing(wmd_handle* h, int enable);
+wmd_status wmd_stage_times(wmd_handle* h, float* select_ms, float* cdist_ms,
+                           float* solve_ms);
+
+/* ---------------------------------------------------------------------------
+ * Diagnostics.
+ * ------------------------------------------------------------------------ */
+const char* wmd_status_string(wmd_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* wmd_last_error(void);
+int wmd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WMD_B200_H */

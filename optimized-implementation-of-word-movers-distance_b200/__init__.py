@@ -1,0 +1,223 @@
+"""B200 Sinkhorn Word Mover's Distance engine — host-side Python layer.
+
+Everything here marshals arguments into the C ABI of libwmd_b200.so
+(include/wmd_b200.h); every solve runs in the library's CUDA kernels.
+
+Reference interfaces mirrored:
+
+* ``sinkhorn_wmd(r, c, vecs, lamb, max_iter)`` — the Python reference
+  ``main.py:37-86`` (same arguments, same ``lamb`` sign convention
+  K = exp(M * lamb) of ``main.py:65``, same 1 x N matrix result).
+* ``sinkhorn_wmd_fused`` / ``sinkhorn_wmd_nonfused`` — the C++ solvers
+  ``sinkhorn_wmd_fused.cpp:112`` / ``sinkhorn_wmd_nonfused.cpp:114`` with their
+  own ``lamda`` conventions (exp(M*lamda) and exp(-M*lamda) respectively) and
+  the word-major CSR the reference keeps in its global ``c_csr``.
+* ``Engine`` — the resident-corpus handle API (no reference counterpart).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import synth  # noqa: F401
+from ._native import (  # noqa: F401
+    CDIST_MODES, CSC, CSR, WMDError, check, exported_names, lib, LIB_PATH)
+
+__all__ = ["sinkhorn_wmd", "sinkhorn_wmd_fused", "sinkhorn_wmd_nonfused",
+           "sinkhorn_wmd_csc", "Engine", "WMDError", "synth"]
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _u64(a):
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _csc_struct(V, N, col_ptr, row_inds, vals):
+    keep = (col_ptr, row_inds, vals)
+    s = CSC(V, N, int(col_ptr[-1]), _ptr(col_ptr, ctypes.c_uint64),
+            _ptr(row_inds, ctypes.c_uint64), _ptr(vals, ctypes.c_double))
+    return s, keep
+
+
+def _csr_struct(V, N, row_ptr, col_inds, vals):
+    keep = (row_ptr, col_inds, vals)
+    s = CSR(V, N, int(row_ptr[-1]), _ptr(row_ptr, ctypes.c_uint64),
+            _ptr(col_inds, ctypes.c_uint64), _ptr(vals, ctypes.c_double))
+    return s, keep
+
+
+def sinkhorn_wmd_csc(r, vecs, col_ptr, row_inds, vals, lamda, max_iter,
+                     variant="fused"):
+    """Drop-in solve with a document-major (CSC) target matrix.  ``lamda``
+    follows the chosen reference variant's sign convention."""
+    r, vecs = _f64(r), _f64(vecs)
+    col_ptr, row_inds, vals = _u64(col_ptr), _u64(row_inds), _f64(vals)
+    V, d = vecs.shape
+    N = col_ptr.size - 1
+    out = np.empty(N, np.float64)
+    s, _keep = _csc_struct(V, N, col_ptr, row_inds, vals)
+    fn = (lib().wmd_sinkhorn_fused_csc if variant == "fused"
+          else lib().wmd_sinkhorn_nonfused_csc)
+    check(fn(_ptr(r, ctypes.c_double), _ptr(vecs, ctypes.c_double),
+             _ptr(out, ctypes.c_double), float(lamda), int(max_iter), V, N, d,
+             ctypes.byref(s)))
+    return out
+
+
+def _csr_call(fn, r, vecs, lamda, max_iter, row_ptr, col_inds, vals, num_docs):
+    r, vecs = _f64(r), _f64(vecs)
+    row_ptr, col_inds, vals = _u64(row_ptr), _u64(col_inds), _f64(vals)
+    V, d = vecs.shape
+    out = np.empty(int(num_docs), np.float64)
+    s, _keep = _csr_struct(V, int(num_docs), row_ptr, col_inds, vals)
+    check(fn(_ptr(r, ctypes.c_double), _ptr(vecs, ctypes.c_double),
+             _ptr(out, ctypes.c_double), float(lamda), int(max_iter), V,
+             int(num_docs), d, ctypes.byref(s)))
+    return out
+
+
+def sinkhorn_wmd_fused(r, vecs, lamda, max_iter, row_ptr, col_inds, vals,
+                       num_docs):
+    """Mirror of sinkhorn_wmd (sinkhorn_wmd_fused.cpp:112): K = exp(lamda*M),
+    target matrix as the reference's word-major CSR."""
+    return _csr_call(lib().wmd_sinkhorn_fused, r, vecs, lamda, max_iter,
+                     row_ptr, col_inds, vals, num_docs)
+
+
+def sinkhorn_wmd_nonfused(r, vecs, lamda, max_iter, row_ptr, col_inds, vals,
+                          num_docs):
+    """Mirror of sinkhorn_wmd (sinkhorn_wmd_nonfused.cpp:114):
+    K = exp(-lamda*M)."""
+    return _csr_call(lib().wmd_sinkhorn_nonfused, r, vecs, lamda, max_iter,
+                     row_ptr, col_inds, vals, num_docs)
+
+
+def sinkhorn_wmd(r, c, vecs, lamb, max_iter):
+    """Drop-in for main.py:37 ``sinkhorn_wmd(r, c, vecs, lamb, max_iter)``.
+
+    r: dense query histogram (V,), c: scipy sparse V x N target matrix,
+    vecs: V x d embeddings, lamb: K = exp(M * lamb) (main.py:65; the
+    reference's default is -1).  Returns a 1 x N ``np.matrix`` as main.py's
+    ``(u * ((KM) @ v)).sum(axis=0)`` does.  main.py selects r > 0
+    (main.py:49); negative weights are rejected here, as the reference's C++
+    driver rejects them (sinkhorn_wmd_fused.cpp:570-574).
+    """
+    from scipy import sparse
+    c = sparse.csc_matrix(c)
+    c.sort_indices()
+    r = np.asarray(r, dtype=np.float64).reshape(-1)
+    out = sinkhorn_wmd_csc(r, np.asarray(vecs), c.indptr, c.indices, c.data,
+                           lamb, max_iter, "fused")
+    return np.asmatrix(out.reshape(1, -1))
+
+
+class Engine:
+    """Resident-corpus solver (handle API of include/wmd_b200.h).  ``lam`` is
+    the positive regulariser: K = exp(-lam * M)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        check(lib().wmd_create(ctypes.byref(self._h), int(device)))
+        self.V = self.d = self.N = 0
+
+    def close(self):
+        if self._h:
+            lib().wmd_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return int(lib().wmd_stream(self._h) or 0)
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().wmd_last_launch_count(self._h))
+
+    def set_embeddings(self, vecs):
+        """vecs: numpy float64/float32 (V, d), or a CUDA tensor (torch) of
+        either dtype on this handle's device."""
+        if hasattr(vecs, "data_ptr") and getattr(vecs, "is_cuda", False):
+            V, d = vecs.shape
+            ptr = ctypes.c_void_p(vecs.contiguous().data_ptr())
+            f = (lib().wmd_set_embeddings_f64 if str(vecs.dtype) == "torch.float64"
+                 else lib().wmd_set_embeddings_f32)
+            check(f(self._h, ptr, V, d, 1))
+        else:
+            a = np.asarray(vecs)
+            if a.dtype == np.float32:
+                a = np.ascontiguousarray(a)
+                check(lib().wmd_set_embeddings_f32(
+                    self._h, a.ctypes.data_as(ctypes.c_void_p), a.shape[0],
+                    a.shape[1], 0))
+            else:
+                a = _f64(a)
+                check(lib().wmd_set_embeddings_f64(
+                    self._h, a.ctypes.data_as(ctypes.c_void_p), a.shape[0],
+                    a.shape[1], 0))
+            V, d = a.shape
+        self.V, self.d = int(V), int(d)
+
+    def set_targets(self, col_ptr, row_inds, vals, V=None):
+        col_ptr, row_inds, vals = _u64(col_ptr), _u64(row_inds), _f64(vals)
+        V = self.V if V is None else int(V)
+        N = col_ptr.size - 1
+        s, _keep = _csc_struct(V, N, col_ptr, row_inds, vals)
+        check(lib().wmd_set_targets_csc(self._h, ctypes.byref(s)))
+        self.N = N
+
+    def set_targets_csr(self, row_ptr, col_inds, vals, N):
+        row_ptr, col_inds, vals = _u64(row_ptr), _u64(col_inds), _f64(vals)
+        V = row_ptr.size - 1
+        s, _keep = _csr_struct(V, int(N), row_ptr, col_inds, vals)
+        check(lib().wmd_set_targets_csr(self._h, ctypes.byref(s)))
+        self.N = int(N)
+
+    def set_cdist_mode(self, mode: str):
+        check(lib().wmd_set_cdist_mode(self._h, CDIST_MODES[mode]))
+
+    def query(self, r, lam: float, max_iter: int) -> np.ndarray:
+        r = _f64(r)
+        out = np.empty(self.N, np.float64)
+        check(lib().wmd_query_dense(self._h, _ptr(r, ctypes.c_double),
+                                    float(lam), int(max_iter),
+                                    _ptr(out, ctypes.c_double)))
+        return out
+
+    def query_device(self, r_dev_ptr: int, vr_cap: int, lam: float,
+                     max_iter: int, out_dev_ptr: int):
+        """Asynchronous solve on device pointers (e.g. torch ``data_ptr()``)
+        on the handle's stream; call ``check()`` to synchronise."""
+        check(lib().wmd_query_dense_device(
+            self._h, ctypes.c_void_p(r_dev_ptr), int(vr_cap), float(lam),
+            int(max_iter), ctypes.c_void_p(out_dev_ptr)))
+
+    def check(self):
+        check(lib().wmd_check(self._h))
+
+    def set_timing(self, enable: bool = True):
+        check(lib().wmd_set_timing(self._h, int(bool(enable))))
+
+    def stage_times(self):
+        """(select_ms, cdist_ms, solve_ms) of the last query (synchronises)."""
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        check(lib().wmd_stage_times(self._h, ctypes.byref(a), ctypes.byref(b),
+                                    ctypes.byref(c)))
+        return a.value, b.value, c.value

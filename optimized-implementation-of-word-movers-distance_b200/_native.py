@@ -1,0 +1,113 @@
+"""ctypes binding of libwmd_b200.so (the C ABI declared in include/wmd_b200.h).
+
+Loading fails loudly when the library is missing: there is no Python or CPU
+fallback for any solve.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwmd_b200.so")
+
+c_u64 = ctypes.c_uint64
+c_f64p = ctypes.POINTER(ctypes.c_double)
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+STATUS = {
+    0: "WMD_OK", 1: "WMD_ERR_INVALID_ARG", 2: "WMD_ERR_INVALID_INPUT",
+    3: "WMD_ERR_OUT_OF_MEMORY", 4: "WMD_ERR_CUDA", 5: "WMD_ERR_NO_DEVICE",
+    6: "WMD_ERR_UNSUPPORTED",
+}
+
+CDIST_MODES = {"fp32": 0, "bf16": 1, "fp16": 2}
+
+
+class WMDError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.name = STATUS.get(status, f"status {status}")
+        super().__init__(f"{self.name}: {message}")
+
+
+class CSR(ctypes.Structure):
+    """Mirror of puma_csr_double_t (common.h:38-46)."""
+    _fields_ = [("num_rows", c_u64), ("num_cols", c_u64), ("nnz", c_u64),
+                ("row_ptr", c_u64p), ("col_inds", c_u64p), ("vals", c_f64p)]
+
+
+class CSC(ctypes.Structure):
+    """Mirror of puma_csc_double_t (common.h:49-57)."""
+    _fields_ = [("num_rows", c_u64), ("num_cols", c_u64), ("nnz", c_u64),
+                ("col_ptr", c_u64p), ("row_inds", c_u64p), ("vals", c_f64p)]
+
+
+# (name, restype, argtypes) for every entry point of include/wmd_b200.h.
+_SIGS = [
+    ("wmd_sinkhorn_fused", ctypes.c_int,
+     [c_f64p, c_f64p, c_f64p, ctypes.c_double, ctypes.c_int, c_u64, c_u64,
+      c_u64, ctypes.POINTER(CSR)]),
+    ("wmd_sinkhorn_nonfused", ctypes.c_int,
+     [c_f64p, c_f64p, c_f64p, ctypes.c_double, ctypes.c_int, c_u64, c_u64,
+      c_u64, ctypes.POINTER(CSR)]),
+    ("wmd_sinkhorn_fused_csc", ctypes.c_int,
+     [c_f64p, c_f64p, c_f64p, ctypes.c_double, ctypes.c_int, c_u64, c_u64,
+      c_u64, ctypes.POINTER(CSC)]),
+    ("wmd_sinkhorn_nonfused_csc", ctypes.c_int,
+     [c_f64p, c_f64p, c_f64p, ctypes.c_double, ctypes.c_int, c_u64, c_u64,
+      c_u64, ctypes.POINTER(CSC)]),
+    ("wmd_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+    ("wmd_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("wmd_set_embeddings_f64", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, ctypes.c_int]),
+    ("wmd_set_embeddings_f32", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, ctypes.c_int]),
+    ("wmd_set_targets_csc", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSC)]),
+    ("wmd_set_targets_csr", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSR)]),
+    ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_query_dense", ctypes.c_int,
+     [ctypes.c_void_p, c_f64p, ctypes.c_double, ctypes.c_int, c_f64p]),
+    ("wmd_query_dense_device", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, c_u64, ctypes.c_double, ctypes.c_int,
+      ctypes.c_void_p]),
+    ("wmd_check", ctypes.c_int, [ctypes.c_void_p]),
+    ("wmd_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("wmd_last_launch_count", ctypes.c_int, [ctypes.c_void_p]),
+    ("wmd_set_timing", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_stage_times", ctypes.c_int,
+     [ctypes.c_void_p, c_f32p, c_f32p, c_f32p]),
+    ("wmd_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("wmd_last_error", ctypes.c_char_p, []),
+    ("wmd_abi_version", ctypes.c_int, []),
+]
+
+_lib = None
+
+
+def lib():
+    """Load libwmd_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with "
+                f"`python {os.path.join(HERE, 'build.py')}`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _SIGS:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_names():
+    return [s[0] for s in _SIGS]
+
+
+def check(status: int):
+    if status != 0:
+        msg = lib().wmd_last_error().decode(errors="replace")
+        raise WMDError(status, msg)

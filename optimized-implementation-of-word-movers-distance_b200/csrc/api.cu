@@ -1,0 +1,635 @@
+// C ABI (include/wmd_b200.h): handles, device buffers, validation and the
+// drop-in replacements of the reference's sinkhorn_wmd.
+//
+// Every solve runs on the GPU.  There is no host fallback: if the device or a
+// kernel launch fails, the call returns an error status.
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "wmd_b200.h"
+#include "wmd_internal.cuh"
+
+using namespace wmd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+wmd_status fail(wmd_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+wmd_status fail_cuda(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky launch error where possible
+  const wmd_status s =
+      e == cudaErrorMemoryAllocation ? WMD_ERR_OUT_OF_MEMORY : WMD_ERR_CUDA;
+  return fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return fail_cuda(e_, #call);   \
+  } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = bytes ? bytes : 16;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+std::string describe_err_bits(unsigned bits) {
+  std::string s;
+  if (bits & ERR_ROW_RANGE) s += " word index >= vocabulary size;";
+  if (bits & ERR_COLPTR) s += " column pointers not monotone from 0 to nnz;";
+  if (bits & ERR_NEG_R) s += " negative source weight;";
+  if (bits & ERR_BAD_VAL) s += " target value <= 0 or not finite;";
+  if (bits & ERR_VR_CAP) s += " more non-zero source words than vr_cap;";
+  return s;
+}
+
+}  // namespace
+
+struct wmd_handle {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  wmd_cdist_mode mode = WMD_CDIST_FP32;
+  // embeddings
+  DevBuf E32, nE, E64_stage;
+  uint64_t V = 0, d = 0;
+  bool have_E = false;
+  // targets
+  DevBuf col_ptr, ent, order, stage_cp, stage_rows, stage_vals;
+  uint64_t tV = 0, N = 0, nnz = 0;
+  bool have_T = false;
+  // per query
+  DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_vr, sel_chunks, K, KM,
+      out_dev, err_dev;
+  unsigned* err_host = nullptr;      // pinned
+  uint32_t* chunks_host = nullptr;   // pinned, grown with V
+  size_t chunks_host_cap = 0;
+  int last_launches = 0;
+  // stage timing
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+wmd_status bind(wmd_handle* h) {
+  CK(cudaSetDevice(h->device));
+  return WMD_OK;
+}
+
+wmd_status clear_err(wmd_handle* h) {
+  CK(cudaMemsetAsync(h->err_dev.p, 0, sizeof(unsigned), h->stream));
+  return WMD_OK;
+}
+
+// Synchronise and turn device-side validation bits into a status.
+wmd_status finish(wmd_handle* h) {
+  CK(cudaMemcpyAsync(h->err_host, h->err_dev.p, sizeof(unsigned),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  const unsigned bits = *h->err_host;
+  if (bits) {
+    clear_err(h);
+    return fail(WMD_ERR_INVALID_INPUT, "invalid input:" + describe_err_bits(bits));
+  }
+  return WMD_OK;
+}
+
+wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
+                          uint64_t d, int where, bool f64) {
+  if (!h || !vecs || V == 0 || d == 0 || (where != 0 && where != 1))
+    return fail(WMD_ERR_INVALID_ARG, "set_embeddings: bad argument");
+  if (V > 0xFFFFFFFFull)
+    return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^32 words");
+  wmd_status s = bind(h);
+  if (s) return s;
+  const size_t n = (size_t)V * d;
+  CK(h->E32.ensure(n * sizeof(float)));
+  CK(h->nE.ensure((size_t)V * sizeof(float)));
+  int launches = 0;
+  if (f64) {
+    const double* src = static_cast<const double*>(vecs);
+    if (where == 0) {
+      CK(h->E64_stage.ensure(n * sizeof(double)));
+      CK(cudaMemcpyAsync(h->E64_stage.p, vecs, n * sizeof(double),
+                         cudaMemcpyHostToDevice, h->stream));
+      src = h->E64_stage.as<double>();
+    }
+    launches += launch_embed_convert_f64(src, V, d, h->E32.as<float>(),
+                                         h->nE.as<float>(), h->stream);
+  } else {
+    CK(cudaMemcpyAsync(h->E32.p, vecs, n * sizeof(float),
+                       where == 0 ? cudaMemcpyHostToDevice
+                                  : cudaMemcpyDeviceToDevice,
+                       h->stream));
+    launches += launch_embed_norms(h->E32.as<float>(), V, d, h->nE.as<float>(),
+                                   h->stream);
+  }
+  CK(cudaGetLastError());
+  h->V = V;
+  h->d = d;
+  h->have_E = true;
+  h->last_launches = launches;
+  return WMD_OK;
+}
+
+// Host-side permutation of the documents by decreasing length (a counting
+// sort on lengths), used by the solver to balance its persistent warps.
+void length_order(const uint64_t* col_ptr, uint64_t N, std::vector<int32_t>& ord) {
+  uint64_t maxlen = 0;
+  for (uint64_t j = 0; j < N; ++j) maxlen = std::max(maxlen, col_ptr[j + 1] - col_ptr[j]);
+  const uint64_t nb = std::min<uint64_t>(maxlen, 1u << 20) + 1;
+  std::vector<uint64_t> cnt(nb + 1, 0);
+  auto bucket = [&](uint64_t j) {
+    const uint64_t l = col_ptr[j + 1] - col_ptr[j];
+    return nb - 1 - std::min<uint64_t>(l, nb - 1);  // longest first
+  };
+  for (uint64_t j = 0; j < N; ++j) cnt[bucket(j) + 1]++;
+  for (uint64_t b = 0; b < nb; ++b) cnt[b + 1] += cnt[b];
+  ord.resize(N);
+  for (uint64_t j = 0; j < N; ++j) ord[cnt[bucket(j)]++] = (int32_t)j;
+}
+
+wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
+  if (!h || !c) return fail(WMD_ERR_INVALID_ARG, "set_targets: null argument");
+  const uint64_t V = c->num_rows, N = c->num_cols, nnz = c->nnz;
+  if (V == 0 || N == 0)
+    return fail(WMD_ERR_INVALID_INPUT, "target matrix has no rows or columns");
+  if (nnz == 0)  // the reference driver rejects an empty matrix (fused:431-435)
+    return fail(WMD_ERR_INVALID_INPUT, "target matrix has no non-zeros");
+  if (!c->col_ptr || !c->row_inds || !c->vals)
+    return fail(WMD_ERR_INVALID_ARG, "target matrix has null arrays");
+  if (N >= 0x7FFFFFFFull)
+    return fail(WMD_ERR_UNSUPPORTED, "more than 2^31-1 target documents");
+  if (c->col_ptr[N] != nnz || c->col_ptr[0] != 0)
+    return fail(WMD_ERR_INVALID_INPUT, "column pointers do not span [0, nnz]");
+  for (uint64_t j = 0; j < N; ++j)
+    if (c->col_ptr[j + 1] < c->col_ptr[j])
+      return fail(WMD_ERR_INVALID_INPUT, "column pointers decrease");
+  wmd_status s = bind(h);
+  if (s) return s;
+  std::vector<int32_t> ord;
+  length_order(c->col_ptr, N, ord);
+  CK(h->stage_cp.ensure((N + 1) * sizeof(uint64_t)));
+  CK(h->stage_rows.ensure(nnz * sizeof(uint64_t)));
+  CK(h->stage_vals.ensure(nnz * sizeof(double)));
+  CK(h->col_ptr.ensure((N + 1) * sizeof(int64_t)));
+  CK(h->ent.ensure(nnz * sizeof(uint2)));
+  CK(h->order.ensure(N * sizeof(int32_t)));
+  CK(cudaMemcpyAsync(h->stage_cp.p, c->col_ptr, (N + 1) * sizeof(uint64_t),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->stage_rows.p, c->row_inds, nnz * sizeof(uint64_t),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->stage_vals.p, c->vals, nnz * sizeof(double),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->order.p, ord.data(), N * sizeof(int32_t),
+                     cudaMemcpyHostToDevice, h->stream));
+  s = clear_err(h);
+  if (s) return s;
+  const int launches = launch_pack_targets(
+      h->stage_cp.as<uint64_t>(), h->stage_rows.as<uint64_t>(),
+      h->stage_vals.as<double>(), V, N, nnz, h->col_ptr.as<int64_t>(),
+      h->ent.as<uint2>(), h->err_dev.as<unsigned>(), h->stream);
+  CK(cudaGetLastError());
+  h->have_T = false;
+  s = finish(h);  // the order vector must outlive its async copy
+  if (s) return s;
+  h->tV = V;
+  h->N = N;
+  h->nnz = nnz;
+  h->have_T = true;
+  h->last_launches = launches;
+  return WMD_OK;
+}
+
+// Stable CSR (rows = words) -> CSC (columns = documents) transpose, the
+// counting sort of sinkhorn_wmd_fused.cpp:493-506 keyed by document: within a
+// document, entries come out in ascending word order (equal words keep their
+// CSR order), which is the order the reference accumulates in on one thread.
+wmd_status csr_to_csc_host(const wmd_csr_double_t* a, std::vector<uint64_t>& cp,
+                           std::vector<uint64_t>& rows, std::vector<double>& vals) {
+  const uint64_t V = a->num_rows, N = a->num_cols, nnz = a->nnz;
+  if (!a->row_ptr || !a->col_inds || !a->vals)
+    return fail(WMD_ERR_INVALID_ARG, "target matrix has null arrays");
+  if (a->row_ptr[0] != 0 || a->row_ptr[V] != nnz)
+    return fail(WMD_ERR_INVALID_INPUT, "row pointers do not span [0, nnz]");
+  cp.assign(N + 1, 0);
+  for (uint64_t w = 0; w < V; ++w) {
+    if (a->row_ptr[w + 1] < a->row_ptr[w])
+      return fail(WMD_ERR_INVALID_INPUT, "row pointers decrease");
+  }
+  for (uint64_t e = 0; e < nnz; ++e) {
+    const uint64_t j = a->col_inds[e];
+    if (j >= N) return fail(WMD_ERR_INVALID_INPUT, "document index >= num_cols");
+    cp[j + 1]++;
+  }
+  for (uint64_t j = 0; j < N; ++j) cp[j + 1] += cp[j];
+  std::vector<uint64_t> fill(cp.begin(), cp.end() - 1);
+  rows.resize(nnz);
+  vals.resize(nnz);
+  for (uint64_t w = 0; w < V; ++w)
+    for (uint64_t e = a->row_ptr[w]; e < a->row_ptr[w + 1]; ++e) {
+      const uint64_t pos = fill[a->col_inds[e]]++;
+      rows[pos] = w;
+      vals[pos] = a->vals[e];
+    }
+  return WMD_OK;
+}
+
+// One query on device-resident r.  cap bounds v_r.  expo: K = exp(expo * M).
+wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
+                        float expo, int max_iter, double* out_dev) {
+  const uint64_t V = h->V, d = h->d;
+  const int nchunks = select_num_chunks(V);
+  const int ld = (int)(((cap ? cap : 1) + 3u) & ~3u);
+  CK(h->sel_ids.ensure((size_t)std::max<uint32_t>(cap, 1) * sizeof(uint32_t)));
+  CK(h->sel_rinv.ensure((size_t)std::max<uint32_t>(cap, 1) * sizeof(float)));
+  CK(h->sel_S.ensure((size_t)std::max<uint32_t>(cap, 1) * d * sizeof(float)));
+  CK(h->sel_nS.ensure((size_t)std::max<uint32_t>(cap, 1) * sizeof(float)));
+  CK(h->sel_vr.ensure(sizeof(uint32_t)));
+  CK(h->sel_chunks.ensure((size_t)nchunks * sizeof(uint32_t)));
+  CK(h->K.ensure((size_t)V * ld * sizeof(float)));
+  CK(h->KM.ensure((size_t)V * ld * sizeof(float)));
+  SourceSel sel;
+  sel.ids = h->sel_ids.as<uint32_t>();
+  sel.rinv = h->sel_rinv.as<float>();
+  sel.S = h->sel_S.as<float>();
+  sel.nS = h->sel_nS.as<float>();
+  sel.vr = h->sel_vr.as<uint32_t>();
+  sel.chunk_counts = h->sel_chunks.as<uint32_t>();
+  sel.cap = cap;
+  Targets t;
+  t.col_ptr = h->col_ptr.as<int64_t>();
+  t.ent = h->ent.as<uint2>();
+  t.order = h->order.as<int32_t>();
+  t.N = (int64_t)h->N;
+  t.nnz = (int64_t)h->nnz;
+  if (h->mode != WMD_CDIST_FP32)
+    return fail(WMD_ERR_UNSUPPORTED, "tensor-core cdist is not built in");
+  if (cap > 1024)
+    return fail(WMD_ERR_UNSUPPORTED, "more than 1024 non-zero source words");
+  int launches = 0;
+  if (h->timing) CK(cudaEventRecord(h->ev[0], h->stream));
+  launches += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d,
+                            sel, h->err_dev.as<unsigned>(), h->stream);
+  if (h->timing) CK(cudaEventRecord(h->ev[1], h->stream));
+  launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d, sel,
+                                expo, h->K.as<float>(), h->KM.as<float>(), ld,
+                                h->stream);
+  if (h->timing) CK(cudaEventRecord(h->ev[2], h->stream));
+  launches += launch_solve(h->K.as<float>(), h->KM.as<float>(), ld, cap, sel, t,
+                           max_iter, out_dev, h->stream);
+  if (h->timing) CK(cudaEventRecord(h->ev[3], h->stream));
+  CK(cudaGetLastError());
+  h->last_launches = launches;
+  return WMD_OK;
+}
+
+// Query from a dense HOST histogram: copy, count the non-zeros on the GPU,
+// size the panels for exactly that many source words, solve, copy back.
+wmd_status query_host(wmd_handle* h, const double* r, float expo, int max_iter,
+                      double* wmd_out) {
+  if (!h->have_E || !h->have_T)
+    return fail(WMD_ERR_INVALID_ARG, "embeddings and targets must be set first");
+  if (h->tV != h->V)
+    return fail(WMD_ERR_INVALID_ARG, "target rows != vocabulary size");
+  if (max_iter < 0) return fail(WMD_ERR_INVALID_ARG, "max_iter < 0");
+  const uint64_t V = h->V;
+  const int nchunks = select_num_chunks(V);
+  CK(h->r_dev.ensure(V * sizeof(double)));
+  CK(h->sel_chunks.ensure((size_t)nchunks * sizeof(uint32_t)));
+  CK(h->out_dev.ensure(h->N * sizeof(double)));
+  if (h->chunks_host_cap < (size_t)nchunks) {
+    if (h->chunks_host) cudaFreeHost(h->chunks_host);
+    h->chunks_host = nullptr;
+    h->chunks_host_cap = 0;
+    CK(cudaMallocHost(&h->chunks_host, (size_t)nchunks * sizeof(uint32_t)));
+    h->chunks_host_cap = nchunks;
+  }
+  wmd_status s = clear_err(h);
+  if (s) return s;
+  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice,
+                     h->stream));
+  // Count pass alone first: v_r sizes every later buffer.
+  uint32_t* counts = h->sel_chunks.as<uint32_t>();
+  const int lc = launch_select_count(h->r_dev.as<double>(), V, counts,
+                                     h->err_dev.as<unsigned>(), h->stream);
+  CK(cudaMemcpyAsync(h->chunks_host, counts,
+                     (size_t)nchunks * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                     h->stream));
+  s = finish(h);
+  if (s) return s;
+  uint64_t vr = 0;
+  for (int c = 0; c < nchunks; ++c) vr += h->chunks_host[c];
+  s = query_device(h, h->r_dev.as<double>(), (uint32_t)vr, expo, max_iter,
+                   h->out_dev.as<double>());
+  if (s) return s;
+  h->last_launches += lc;
+  CK(cudaMemcpyAsync(wmd_out, h->out_dev.p, h->N * sizeof(double),
+                     cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+// Per-host-thread default handle for the drop-in calls.
+struct TlHandle {
+  wmd_handle* h = nullptr;
+  ~TlHandle() {
+    if (h) wmd_destroy(h);
+  }
+};
+thread_local TlHandle tl_handle;
+
+wmd_status default_handle(wmd_handle** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (tl_handle.h && tl_handle.h->device != dev) {
+    wmd_destroy(tl_handle.h);
+    tl_handle.h = nullptr;
+  }
+  if (!tl_handle.h) {
+    wmd_status s = wmd_create(&tl_handle.h, dev);
+    if (s) return s;
+  }
+  *out = tl_handle.h;
+  return WMD_OK;
+}
+
+wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
+                      float expo, int max_iter, uint64_t V, uint64_t N,
+                      uint64_t d, const wmd_csc_double_t* c) {
+  if (!r || !vecs || !WMD || !c)
+    return fail(WMD_ERR_INVALID_ARG, "null argument");
+  if (V == 0 || N == 0 || d == 0)
+    return fail(WMD_ERR_INVALID_INPUT, "zero vocabulary, document count or width");
+  if (c->num_rows != V || c->num_cols != N)
+    return fail(WMD_ERR_INVALID_ARG, "matrix shape does not match V x num_docs");
+  if (max_iter < 0) return fail(WMD_ERR_INVALID_ARG, "max_iter < 0");
+  wmd_handle* h = nullptr;
+  wmd_status s = default_handle(&h);
+  if (s) return s;
+  s = set_embeddings(h, vecs, V, d, 0, true);
+  if (s) return s;
+  const int le = h->last_launches;
+  s = set_targets_csc(h, c);
+  if (s) return s;
+  const int lt = h->last_launches;
+  s = query_host(h, r, expo, max_iter, WMD);
+  if (s) return s;
+  h->last_launches += le + lt;
+  return WMD_OK;
+}
+
+wmd_status dropin_csr(const double* r, const double* vecs, double* WMD,
+                      float expo, int max_iter, uint64_t V, uint64_t N,
+                      uint64_t d, const wmd_csr_double_t* a) {
+  if (!a) return fail(WMD_ERR_INVALID_ARG, "null matrix");
+  if (a->num_rows != V || a->num_cols != N)
+    return fail(WMD_ERR_INVALID_ARG, "matrix shape does not match V x num_docs");
+  if (a->nnz == 0)
+    return fail(WMD_ERR_INVALID_INPUT, "target matrix has no non-zeros");
+  std::vector<uint64_t> cp, rows;
+  std::vector<double> vals;
+  wmd_status s = csr_to_csc_host(a, cp, rows, vals);
+  if (s) return s;
+  wmd_csc_double_t c;
+  c.num_rows = V;
+  c.num_cols = N;
+  c.nnz = a->nnz;
+  c.col_ptr = cp.data();
+  c.row_inds = rows.data();
+  c.vals = vals.data();
+  return dropin_csc(r, vecs, WMD, expo, max_iter, V, N, d, &c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int wmd_abi_version(void) { return WMD_B200_ABI_VERSION; }
+
+const char* wmd_status_string(wmd_status s) {
+  switch (s) {
+    case WMD_OK: return "ok";
+    case WMD_ERR_INVALID_ARG: return "invalid argument";
+    case WMD_ERR_INVALID_INPUT: return "invalid input data";
+    case WMD_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case WMD_ERR_CUDA: return "CUDA error";
+    case WMD_ERR_NO_DEVICE: return "no CUDA device";
+    case WMD_ERR_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+const char* wmd_last_error(void) { return g_last_error.c_str(); }
+
+wmd_status wmd_create(wmd_handle** out, int device) {
+  if (!out) return fail(WMD_ERR_INVALID_ARG, "wmd_create: null out");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(WMD_ERR_NO_DEVICE, "no CUDA device visible");
+  }
+  if (device < 0 || device >= n)
+    return fail(WMD_ERR_INVALID_ARG, "wmd_create: device out of range");
+  wmd_handle* h = new wmd_handle();
+  h->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = h->err_dev.ensure(sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(h->err_dev.p, 0, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMallocHost(&h->err_host, sizeof(unsigned));
+  for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  if (e != cudaSuccess) {
+    wmd_destroy(h);
+    return fail_cuda(e, "wmd_create");
+  }
+  *out = h;
+  return WMD_OK;
+}
+
+wmd_status wmd_destroy(wmd_handle* h) {
+  if (!h) return WMD_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (DevBuf* b : {&h->E32, &h->nE, &h->E64_stage, &h->col_ptr, &h->ent,
+                    &h->order, &h->stage_cp, &h->stage_rows, &h->stage_vals,
+                    &h->r_dev, &h->sel_ids, &h->sel_rinv, &h->sel_S, &h->sel_nS,
+                    &h->sel_vr, &h->sel_chunks, &h->K, &h->KM, &h->out_dev,
+                    &h->err_dev})
+    b->release();
+  if (h->err_host) cudaFreeHost(h->err_host);
+  if (h->chunks_host) cudaFreeHost(h->chunks_host);
+  for (int i = 0; i < 4; ++i)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return WMD_OK;
+}
+
+wmd_status wmd_set_embeddings_f64(wmd_handle* h, const double* vecs, uint64_t V,
+                                  uint64_t d, int where) {
+  return set_embeddings(h, vecs, V, d, where, true);
+}
+
+wmd_status wmd_set_embeddings_f32(wmd_handle* h, const float* vecs, uint64_t V,
+                                  uint64_t d, int where) {
+  return set_embeddings(h, vecs, V, d, where, false);
+}
+
+wmd_status wmd_set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
+  return set_targets_csc(h, c);
+}
+
+wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* a) {
+  if (!h || !a) return fail(WMD_ERR_INVALID_ARG, "set_targets: null argument");
+  if (a->num_rows == 0 || a->num_cols == 0 || a->nnz == 0)
+    return fail(WMD_ERR_INVALID_INPUT, "empty target matrix");
+  std::vector<uint64_t> cp, rows;
+  std::vector<double> vals;
+  wmd_status s = csr_to_csc_host(a, cp, rows, vals);
+  if (s) return s;
+  wmd_csc_double_t c;
+  c.num_rows = a->num_rows;
+  c.num_cols = a->num_cols;
+  c.nnz = a->nnz;
+  c.col_ptr = cp.data();
+  c.row_inds = rows.data();
+  c.vals = vals.data();
+  return set_targets_csc(h, &c);
+}
+
+wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (mode != WMD_CDIST_FP32)
+    return fail(WMD_ERR_UNSUPPORTED, "tensor-core cdist is not built in");
+  h->mode = mode;
+  return WMD_OK;
+}
+
+wmd_status wmd_query_dense(wmd_handle* h, const double* r, double lambda,
+                           int max_iter, double* wmd_out) {
+  if (!h || !r || !wmd_out) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  wmd_status s = bind(h);
+  if (s) return s;
+  return query_host(h, r, (float)(-lambda), max_iter, wmd_out);
+}
+
+wmd_status wmd_query_dense_device(wmd_handle* h, const double* r_dev,
+                                  uint64_t vr_cap, double lambda, int max_iter,
+                                  double* wmd_dev) {
+  if (!h || !r_dev || !wmd_dev) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  if (!h->have_E || !h->have_T)
+    return fail(WMD_ERR_INVALID_ARG, "embeddings and targets must be set first");
+  if (h->tV != h->V)
+    return fail(WMD_ERR_INVALID_ARG, "target rows != vocabulary size");
+  if (max_iter < 0) return fail(WMD_ERR_INVALID_ARG, "max_iter < 0");
+  if (vr_cap > 1024)
+    return fail(WMD_ERR_UNSUPPORTED, "vr_cap above 1024");
+  wmd_status s = bind(h);
+  if (s) return s;
+  return query_device(h, r_dev, (uint32_t)vr_cap, (float)(-lambda), max_iter,
+                      wmd_dev);
+}
+
+wmd_status wmd_check(wmd_handle* h) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  wmd_status s = bind(h);
+  if (s) return s;
+  return finish(h);
+}
+
+void* wmd_stream(wmd_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int wmd_last_launch_count(wmd_handle* h) { return h ? h->last_launches : 0; }
+
+wmd_status wmd_set_timing(wmd_handle* h, int enable) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  h->timing = enable != 0;
+  return WMD_OK;
+}
+
+wmd_status wmd_stage_times(wmd_handle* h, float* select_ms, float* cdist_ms,
+                           float* solve_ms) {
+  if (!h || !select_ms || !cdist_ms || !solve_ms)
+    return fail(WMD_ERR_INVALID_ARG, "null argument");
+  if (!h->timing) return fail(WMD_ERR_INVALID_ARG, "timing is not enabled");
+  wmd_status s = bind(h);
+  if (s) return s;
+  CK(cudaEventSynchronize(h->ev[3]));
+  CK(cudaEventElapsedTime(select_ms, h->ev[0], h->ev[1]));
+  CK(cudaEventElapsedTime(cdist_ms, h->ev[1], h->ev[2]));
+  CK(cudaEventElapsedTime(solve_ms, h->ev[2], h->ev[3]));
+  return WMD_OK;
+}
+
+wmd_status wmd_sinkhorn_fused(const double* r, const double* vecs, double* WMD,
+                              double lamda, int max_iter,
+                              uint64_t data_vocab_size, uint64_t num_docs,
+                              uint64_t word2vec_word_embedding_size,
+                              const wmd_csr_double_t* c_csr) {
+  return dropin_csr(r, vecs, WMD, (float)lamda, max_iter, data_vocab_size,
+                    num_docs, word2vec_word_embedding_size, c_csr);
+}
+
+wmd_status wmd_sinkhorn_nonfused(const double* r, const double* vecs,
+                                 double* WMD, double lamda, int max_iter,
+                                 uint64_t data_vocab_size, uint64_t num_docs,
+                                 uint64_t word2vec_word_embedding_size,
+                                 const wmd_csr_double_t* c_csr) {
+  return dropin_csr(r, vecs, WMD, (float)(-lamda), max_iter, data_vocab_size,
+                    num_docs, word2vec_word_embedding_size, c_csr);
+}
+
+wmd_status wmd_sinkhorn_fused_csc(const double* r, const double* vecs,
+                                  double* WMD, double lamda, int max_iter,
+                                  uint64_t data_vocab_size, uint64_t num_docs,
+                                  uint64_t word2vec_word_embedding_size,
+                                  const wmd_csc_double_t* c_csc) {
+  return dropin_csc(r, vecs, WMD, (float)lamda, max_iter, data_vocab_size,
+                    num_docs, word2vec_word_embedding_size, c_csc);
+}
+
+wmd_status wmd_sinkhorn_nonfused_csc(const double* r, const double* vecs,
+                                     double* WMD, double lamda, int max_iter,
+                                     uint64_t data_vocab_size,
+                                     uint64_t num_docs,
+                                     uint64_t word2vec_word_embedding_size,
+                                     const wmd_csc_double_t* c_csc) {
+  return dropin_csc(r, vecs, WMD, (float)(-lamda), max_iter, data_vocab_size,
+                    num_docs, word2vec_word_embedding_size, c_csc);
+}
+
+}  // extern "C"

@@ -1,0 +1,256 @@
+// Input preparation kernels: embedding conversion, target packing with
+// validation, and source-word selection.
+//
+// Selection restates select_non_empty_entries (sinkhorn_wmd_fused.cpp:45-63):
+// every id with r != 0, in ascending id order, with weight r.  The reference
+// does it serially; here it is a two-launch stream compaction (count per
+// 4096-element chunk, then each chunk scans its flags and writes at the
+// offset of the chunks before it), so the order is the reference's.
+#include "wmd_internal.cuh"
+
+namespace wmd {
+
+// ---------------------------------------------------------------------------
+// Embeddings: FP64 [V][d] -> FP32 [V][d] plus squared norms (one warp per row).
+// ---------------------------------------------------------------------------
+__global__ void embed_convert_f64_kernel(const double* __restrict__ src,
+                                         uint64_t V, uint64_t d,
+                                         float* __restrict__ E32,
+                                         float* __restrict__ nE) {
+  const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= V) return;
+  const double* s = src + row * d;
+  float* o = E32 + row * d;
+  double acc = 0.0;
+  for (uint64_t k = lane; k < d; k += 32) {
+    const float f = (float)s[k];
+    o[k] = f;
+    acc += (double)f * (double)f;
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) nE[row] = (float)acc;
+}
+
+__global__ void embed_norms_kernel(const float* __restrict__ E32, uint64_t V,
+                                   uint64_t d, float* __restrict__ nE) {
+  const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= V) return;
+  const float* s = E32 + row * d;
+  double acc = 0.0;
+  for (uint64_t k = lane; k < d; k += 32) {
+    const double f = (double)s[k];
+    acc += f * f;
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) nE[row] = (float)acc;
+}
+
+int launch_embed_convert_f64(const double* src, uint64_t V, uint64_t d,
+                             float* E32, float* nE, cudaStream_t st) {
+  const int threads = 256;
+  const uint64_t blocks = (V * 32 + threads - 1) / threads;
+  embed_convert_f64_kernel<<<(unsigned)blocks, threads, 0, st>>>(src, V, d, E32, nE);
+  return 1;
+}
+
+int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
+                       cudaStream_t st) {
+  const int threads = 256;
+  const uint64_t blocks = (V * 32 + threads - 1) / threads;
+  embed_norms_kernel<<<(unsigned)blocks, threads, 0, st>>>(E32, V, d, nE);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Targets: validate a CSC triple and pack it for the solver.  The checks are
+// those of the reference driver's MTX reader (sinkhorn_wmd_fused.cpp:474-478):
+// indices in range and values > 0; plus consistent column pointers.
+// ---------------------------------------------------------------------------
+__global__ void pack_colptr_kernel(const uint64_t* __restrict__ cp_in,
+                                   uint64_t N, uint64_t nnz,
+                                   int64_t* __restrict__ cp_out,
+                                   unsigned* __restrict__ err) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > N) return;
+  const uint64_t a = cp_in[j];
+  bool bad = a > nnz;
+  if (j == 0) bad |= (a != 0);
+  if (j == N) bad |= (a != nnz);
+  if (j < N) bad |= (cp_in[j + 1] < a);
+  if (bad) atomicOr(err, ERR_COLPTR);
+  cp_out[j] = (int64_t)(a > nnz ? nnz : a);
+}
+
+__global__ void pack_entries_kernel(const uint64_t* __restrict__ rows,
+                                    const double* __restrict__ vals,
+                                    uint64_t nnz, uint64_t V,
+                                    uint2* __restrict__ ent,
+                                    unsigned* __restrict__ err) {
+  const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nnz) return;
+  uint64_t w = rows[e];
+  const double v = vals[e];
+  unsigned bad = 0;
+  if (w >= V) {
+    bad |= ERR_ROW_RANGE;
+    w = 0;  // keep every later gather in bounds
+  }
+  if (!(v > 0.0) || !isfinite(v)) bad |= ERR_BAD_VAL;
+  if (bad) atomicOr(err, bad);
+  ent[e] = make_uint2((unsigned)w, __float_as_uint((float)v));
+}
+
+int launch_pack_targets(const uint64_t* col_ptr_in, const uint64_t* rows_in,
+                        const double* vals_in, uint64_t V, uint64_t N,
+                        uint64_t nnz, int64_t* col_ptr, uint2* ent,
+                        unsigned* err, cudaStream_t st) {
+  const int threads = 256;
+  pack_colptr_kernel<<<(unsigned)((N + 1 + threads - 1) / threads), threads, 0, st>>>(
+      col_ptr_in, N, nnz, col_ptr, err);
+  int n = 1;
+  if (nnz) {
+    pack_entries_kernel<<<(unsigned)((nnz + threads - 1) / threads), threads, 0, st>>>(
+        rows_in, vals_in, nnz, V, ent, err);
+    n++;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// Source selection.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned block_sum_u32(unsigned v, unsigned* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  unsigned t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0u;
+#pragma unroll
+    for (int off = 16; off; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    if (threadIdx.x == 0) red[32] = t;
+  }
+  __syncthreads();
+  t = red[32];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(kSelectThreads)
+select_count_kernel(const double* __restrict__ r, uint64_t V,
+                    uint32_t* __restrict__ chunk_counts,
+                    unsigned* __restrict__ err) {
+  __shared__ unsigned red[33];
+  const uint64_t base = (uint64_t)blockIdx.x * kSelectChunk;
+  unsigned cnt = 0;
+  bool neg = false;
+#pragma unroll 4
+  for (int k = 0; k < kSelectPerThread; ++k) {
+    const uint64_t i = base + (uint64_t)k * kSelectThreads + threadIdx.x;
+    if (i < V) {
+      const double v = r[i];
+      cnt += (v != 0.0);
+      neg |= (v < 0.0);
+    }
+  }
+  if (neg) atomicOr(err, ERR_NEG_R);
+  const unsigned tot = block_sum_u32(cnt, red);
+  if (threadIdx.x == 0) chunk_counts[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kSelectThreads)
+select_write_kernel(const double* __restrict__ r, uint64_t V,
+                    const float* __restrict__ E32, const float* __restrict__ nE,
+                    uint64_t d, int nchunks,
+                    const uint32_t* __restrict__ chunk_counts,
+                    uint32_t cap, uint32_t* __restrict__ ids,
+                    float* __restrict__ rinv, float* __restrict__ S,
+                    float* __restrict__ nS, uint32_t* __restrict__ vr_out,
+                    unsigned* __restrict__ err) {
+  __shared__ unsigned red[33];
+  __shared__ unsigned warp_off[kSelectThreads / 32];
+  __shared__ uint32_t list_pos[kSelectChunk];
+  __shared__ uint32_t list_id[kSelectChunk];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  // Offset of this chunk = selected count of all chunks before it.
+  unsigned before = 0, all = 0;
+  for (int c = threadIdx.x; c < nchunks; c += blockDim.x) {
+    const unsigned v = chunk_counts[c];
+    all += v;
+    if (c < (int)blockIdx.x) before += v;
+  }
+  const unsigned offset = block_sum_u32(before, red);
+  const unsigned total = block_sum_u32(all, red);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *vr_out = total < cap ? total : cap;
+    if (total > cap) atomicOr(err, ERR_VR_CAP);
+  }
+
+  const uint64_t base = (uint64_t)blockIdx.x * kSelectChunk;
+  unsigned running = 0;
+  for (int k = 0; k < kSelectPerThread; ++k) {
+    const uint64_t i = base + (uint64_t)k * kSelectThreads + threadIdx.x;
+    double v = 0.0;
+    if (i < V) v = r[i];
+    const bool sel = (i < V) && (v != 0.0);
+    const unsigned bal = __ballot_sync(0xffffffffu, sel);
+    if (lane == 0) warp_off[warp] = __popc(bal);
+    __syncthreads();
+    unsigned wpre = 0, ktot = 0;
+#pragma unroll
+    for (int w = 0; w < kSelectThreads / 32; ++w) {
+      const unsigned c = warp_off[w];
+      wpre += (w < warp) ? c : 0u;
+      ktot += c;
+    }
+    if (sel) {
+      const unsigned local = running + wpre + __popc(bal & ((1u << lane) - 1u));
+      const unsigned pos = offset + local;
+      list_pos[local] = pos;
+      list_id[local] = (uint32_t)i;
+      if (pos < cap) {
+        ids[pos] = (uint32_t)i;
+        rinv[pos] = (float)(1.0 / v);
+      }
+    }
+    running += ktot;
+    __syncthreads();
+  }
+  // Gather the selected rows of E32 (one warp per selected word).
+  for (unsigned s = warp; s < running; s += kSelectThreads / 32) {
+    const uint32_t pos = list_pos[s];
+    if (pos >= cap) continue;
+    const uint64_t id = list_id[s];
+    const float* src = E32 + id * d;
+    float* dst = S + (uint64_t)pos * d;
+    for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
+    if (lane == 0) nS[pos] = nE[id];
+  }
+}
+
+int launch_select_count(const double* r, uint64_t V, uint32_t* chunk_counts,
+                        unsigned* err, cudaStream_t st) {
+  select_count_kernel<<<select_num_chunks(V), kSelectThreads, 0, st>>>(
+      r, V, chunk_counts, err);
+  return 1;
+}
+
+int launch_select(const double* r, uint64_t V, const float* E32,
+                  const float* nE, uint64_t d, const SourceSel& s,
+                  unsigned* err, cudaStream_t st) {
+  const int nchunks = select_num_chunks(V);
+  select_count_kernel<<<nchunks, kSelectThreads, 0, st>>>(r, V, s.chunk_counts, err);
+  select_write_kernel<<<nchunks, kSelectThreads, 0, st>>>(
+      r, V, E32, nE, d, nchunks, s.chunk_counts, s.cap, s.ids, s.rinv, s.S,
+      s.nS, s.vr, err);
+  return 2;
+}
+
+}  // namespace wmd

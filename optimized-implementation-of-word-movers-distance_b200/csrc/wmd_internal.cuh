@@ -1,0 +1,89 @@
+// Internal interfaces between the kernels and the C-ABI layer.
+//
+// Device data layout (all row-major, all resident in HBM):
+//   E32   [V][d]    float   embeddings (converted once from the caller's FP64)
+//   nE    [V]       float   squared row norms of E32
+//   E16   [V][dp]   bf16/f16 tensor-core copy of E32, dp = d rounded up to 64
+//   S     [cap][d]  float   embeddings of the selected source words
+//   nS    [cap]     float   their squared norms
+//   K     [V][ld]   float   exp(expo * M) for every (vocabulary word, source word)
+//   KM    [V][ld]   float   K * M (only read by the final half-step)
+//   col_ptr [N+1]   int64   target columns (documents)
+//   ent   [nnz]     uint2   {word id, float bits of the normalised count}
+// ld = number of source words rounded up to a multiple of 4, so that every
+// panel row starts on a 16-byte boundary and is one contiguous gather.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wmd {
+
+// Device-side validation bits, OR-ed into one word per handle.
+enum : unsigned {
+  ERR_ROW_RANGE = 1u,  // word id >= V
+  ERR_COLPTR = 2u,     // column pointers decrease, do not start at 0 or pass nnz
+  ERR_NEG_R = 4u,      // source weight < 0 (the reference driver rejects it)
+  ERR_BAD_VAL = 8u,    // target value <= 0 or not finite
+  ERR_VR_CAP = 16u,    // more selected source words than the panel capacity
+};
+
+constexpr int kSelectThreads = 256;
+constexpr int kSelectPerThread = 16;
+constexpr int kSelectChunk = kSelectThreads * kSelectPerThread;
+
+struct SourceSel {
+  uint32_t* ids = nullptr;     // [cap]
+  float* rinv = nullptr;       // [cap]  1 / r_i
+  float* S = nullptr;          // [cap][d]
+  float* nS = nullptr;         // [cap]
+  uint32_t* vr = nullptr;      // [1]    number of selected words
+  uint32_t* chunk_counts = nullptr;  // [ceil(V / kSelectChunk)]
+  uint32_t cap = 0;
+};
+
+struct Targets {
+  const int64_t* col_ptr = nullptr;
+  const uint2* ent = nullptr;
+  const int32_t* order = nullptr;  // columns by decreasing length (or null)
+  int64_t N = 0;
+  int64_t nnz = 0;
+};
+
+inline int select_num_chunks(uint64_t V) {
+  return (int)((V + kSelectChunk - 1) / kSelectChunk);
+}
+
+// Embeddings: FP64 or FP32 source -> E32 + nE.  Returns launches issued.
+int launch_embed_convert_f64(const double* src, uint64_t V, uint64_t d,
+                             float* E32, float* nE, cudaStream_t st);
+int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
+                       cudaStream_t st);
+
+// Targets: validated packing of a CSC triple into (col_ptr, ent).
+int launch_pack_targets(const uint64_t* col_ptr_in, const uint64_t* rows_in,
+                        const double* vals_in, uint64_t V, uint64_t N,
+                        uint64_t nnz, int64_t* col_ptr, uint2* ent,
+                        unsigned* err, cudaStream_t st);
+
+// Count pass of the selection alone (per-chunk non-zero counts).
+int launch_select_count(const double* r, uint64_t V, uint32_t* chunk_counts,
+                        unsigned* err, cudaStream_t st);
+
+// Source selection r != 0 (ascending id) + gather of the source rows.
+int launch_select(const double* r, uint64_t V, const float* E32,
+                  const float* nE, uint64_t d, const SourceSel& s,
+                  unsigned* err, cudaStream_t st);
+
+// FP32 CUDA-core cost panel: K = exp(expo * M), KM = K * M, M from the GEMM
+// form with near pairs recomputed directly.
+int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
+                      const SourceSel& s, float expo, float* K, float* KM,
+                      int ld, cudaStream_t st);
+
+// Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
+// target document.  Returns launches issued (0 on unsupported vr_cap).
+int launch_solve(const float* K, const float* KM, int ld, uint32_t vr_cap,
+                 const SourceSel& s, const Targets& t, int max_iter,
+                 double* out, cudaStream_t st);
+
+}  // namespace wmd
