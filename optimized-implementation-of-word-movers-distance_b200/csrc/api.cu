@@ -69,6 +69,7 @@ std::string describe_err_bits(unsigned bits) {
   if (bits & ERR_NEG_R) s += " negative source weight;";
   if (bits & ERR_BAD_VAL) s += " target value <= 0 or not finite;";
   if (bits & ERR_VR_CAP) s += " more non-zero source words than vr_cap;";
+  if (bits & ERR_TIMEOUT) s += " device-side wait timed out (kernel aborted);";
   return s;
 }
 
@@ -80,16 +81,17 @@ struct wmd_handle {
   cudaStream_t stream = nullptr;
   wmd_cdist_mode mode = WMD_CDIST_FP32;
   // embeddings
-  DevBuf E32, nE, E64_stage;
+  DevBuf E32, nE, E64_stage, E16;
   uint64_t V = 0, d = 0;
   bool have_E = false;
+  int e16_fmt = -1;  // format E16 holds (1 bf16, 2 fp16), -1 = stale
   // targets
   DevBuf col_ptr, ent, order, stage_cp, stage_rows, stage_vals;
   uint64_t tV = 0, N = 0, nnz = 0;
   bool have_T = false;
   // per query
-  DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_vr, sel_chunks, K, KM,
-      out_dev, err_dev;
+  DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_S16, sel_vr, sel_chunks,
+      K, KM, out_dev, err_dev;
   unsigned* err_host = nullptr;      // pinned
   uint32_t* chunks_host = nullptr;   // pinned, grown with V
   size_t chunks_host_cap = 0;
@@ -159,6 +161,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
   h->V = V;
   h->d = d;
   h->have_E = true;
+  h->e16_fmt = -1;
   h->last_launches = launches;
   return WMD_OK;
 }
@@ -294,18 +297,43 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   t.order = h->order.as<int32_t>();
   t.N = (int64_t)h->N;
   t.nnz = (int64_t)h->nnz;
-  if (h->mode != WMD_CDIST_FP32)
-    return fail(WMD_ERR_UNSUPPORTED, "tensor-core cdist is not built in");
   if (cap > 1024)
     return fail(WMD_ERR_UNSUPPORTED, "more than 1024 non-zero source words");
+  const bool tcm = h->mode != WMD_CDIST_FP32;
+  const bool bf16 = h->mode == WMD_CDIST_BF16;
+  const int dp = tc_padded_width(d);
   int launches = 0;
+  if (tcm) {
+    if (tc_tile_n(cap, d) == 0)
+      return fail(WMD_ERR_UNSUPPORTED, "embedding width too large for the tensor-core panel");
+    const int fmt = bf16 ? 1 : 2;
+    if (h->e16_fmt != fmt) {  // 16-bit copy of the embeddings, built once
+      CK(h->E16.ensure((size_t)V * dp * 2));
+      launches += launch_to16(h->E32.as<float>(), V, d, h->E16.p, bf16, h->stream);
+      h->e16_fmt = fmt;
+    }
+    CK(h->sel_S16.ensure((size_t)std::max<uint32_t>(cap, 1) * dp * 2));
+  }
   if (h->timing) CK(cudaEventRecord(h->ev[0], h->stream));
   launches += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d,
-                            sel, h->err_dev.as<unsigned>(), h->stream);
+                            sel, h->err_dev.as<unsigned>(), h->stream,
+                            tcm ? h->E16.p : nullptr,
+                            tcm ? h->sel_S16.p : nullptr, dp);
   if (h->timing) CK(cudaEventRecord(h->ev[1], h->stream));
-  launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d, sel,
-                                expo, h->K.as<float>(), h->KM.as<float>(), ld,
-                                h->stream);
+  if (tcm) {
+    const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16, h->E32.as<float>(),
+                                   h->nE.as<float>(), V, d, sel, expo,
+                                   h->K.as<float>(), h->KM.as<float>(), ld,
+                                   h->err_dev.as<unsigned>(), h->sms, h->stream);
+    if (lc < 0)
+      return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable "
+                                       "(tensor map encoding failed)");
+    launches += lc;
+  } else {
+    launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d,
+                                  sel, expo, h->K.as<float>(), h->KM.as<float>(),
+                                  ld, h->stream);
+  }
   if (h->timing) CK(cudaEventRecord(h->ev[2], h->stream));
   launches += launch_solve(h->K.as<float>(), h->KM.as<float>(), ld, cap, sel, t,
                            max_iter, out_dev, h->stream);
@@ -484,11 +512,11 @@ wmd_status wmd_destroy(wmd_handle* h) {
   if (!h) return WMD_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (DevBuf* b : {&h->E32, &h->nE, &h->E64_stage, &h->col_ptr, &h->ent,
-                    &h->order, &h->stage_cp, &h->stage_rows, &h->stage_vals,
-                    &h->r_dev, &h->sel_ids, &h->sel_rinv, &h->sel_S, &h->sel_nS,
-                    &h->sel_vr, &h->sel_chunks, &h->K, &h->KM, &h->out_dev,
-                    &h->err_dev})
+  for (DevBuf* b : {&h->E32, &h->nE, &h->E64_stage, &h->E16, &h->col_ptr,
+                    &h->ent, &h->order, &h->stage_cp, &h->stage_rows,
+                    &h->stage_vals, &h->r_dev, &h->sel_ids, &h->sel_rinv,
+                    &h->sel_S, &h->sel_nS, &h->sel_S16, &h->sel_vr,
+                    &h->sel_chunks, &h->K, &h->KM, &h->out_dev, &h->err_dev})
     b->release();
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->chunks_host) cudaFreeHost(h->chunks_host);
@@ -533,8 +561,8 @@ wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* a) {
 
 wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
-  if (mode != WMD_CDIST_FP32)
-    return fail(WMD_ERR_UNSUPPORTED, "tensor-core cdist is not built in");
+  if (mode != WMD_CDIST_FP32 && mode != WMD_CDIST_BF16 && mode != WMD_CDIST_FP16)
+    return fail(WMD_ERR_INVALID_ARG, "unknown cdist mode");
   h->mode = mode;
   return WMD_OK;
 }

@@ -172,7 +172,9 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
                     uint32_t cap, uint32_t* __restrict__ ids,
                     float* __restrict__ rinv, float* __restrict__ S,
                     float* __restrict__ nS, uint32_t* __restrict__ vr_out,
-                    unsigned* __restrict__ err) {
+                    unsigned* __restrict__ err,
+                    const unsigned short* __restrict__ E16,
+                    unsigned short* __restrict__ S16, int dp) {
   __shared__ unsigned red[33];
   __shared__ unsigned warp_off[kSelectThreads / 32];
   __shared__ uint32_t list_pos[kSelectChunk];
@@ -232,6 +234,11 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     float* dst = S + (uint64_t)pos * d;
     for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
     if (lane == 0) nS[pos] = nE[id];
+    if (S16) {  // 16-bit copy for the tensor-core cost panel
+      const unsigned short* s16 = E16 + id * (uint64_t)dp;
+      unsigned short* d16 = S16 + (uint64_t)pos * dp;
+      for (int k = lane; k < dp; k += 32) d16[k] = s16[k];
+    }
   }
 }
 
@@ -244,12 +251,14 @@ int launch_select_count(const double* r, uint64_t V, uint32_t* chunk_counts,
 
 int launch_select(const double* r, uint64_t V, const float* E32,
                   const float* nE, uint64_t d, const SourceSel& s,
-                  unsigned* err, cudaStream_t st) {
+                  unsigned* err, cudaStream_t st, const void* E16, void* S16,
+                  int dp) {
   const int nchunks = select_num_chunks(V);
   select_count_kernel<<<nchunks, kSelectThreads, 0, st>>>(r, V, s.chunk_counts, err);
   select_write_kernel<<<nchunks, kSelectThreads, 0, st>>>(
       r, V, E32, nE, d, nchunks, s.chunk_counts, s.cap, s.ids, s.rinv, s.S,
-      s.nS, s.vr, err);
+      s.nS, s.vr, err, static_cast<const unsigned short*>(E16),
+      static_cast<unsigned short*>(S16), dp);
   return 2;
 }
 

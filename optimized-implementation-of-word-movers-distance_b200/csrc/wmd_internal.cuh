@@ -25,6 +25,7 @@ enum : unsigned {
   ERR_NEG_R = 4u,      // source weight < 0 (the reference driver rejects it)
   ERR_BAD_VAL = 8u,    // target value <= 0 or not finite
   ERR_VR_CAP = 16u,    // more selected source words than the panel capacity
+  ERR_TIMEOUT = 32u,   // a bounded device-side wait gave up (kernel aborted)
 };
 
 constexpr int kSelectThreads = 256;
@@ -69,16 +70,30 @@ int launch_pack_targets(const uint64_t* col_ptr_in, const uint64_t* rows_in,
 int launch_select_count(const double* r, uint64_t V, uint32_t* chunk_counts,
                         unsigned* err, cudaStream_t st);
 
-// Source selection r != 0 (ascending id) + gather of the source rows.
+// Source selection r != 0 (ascending id) + gather of the source rows (and,
+// when S16 is given, of their 16-bit copies [cap][dp] from E16 [V][dp]).
 int launch_select(const double* r, uint64_t V, const float* E32,
                   const float* nE, uint64_t d, const SourceSel& s,
-                  unsigned* err, cudaStream_t st);
+                  unsigned* err, cudaStream_t st, const void* E16 = nullptr,
+                  void* S16 = nullptr, int dp = 0);
 
 // FP32 CUDA-core cost panel: K = exp(expo * M), KM = K * M, M from the GEMM
 // form with near pairs recomputed directly.
 int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
                       const SourceSel& s, float expo, float* K, float* KM,
                       int ld, cudaStream_t st);
+
+// Tensor-core cost panel (cdist_tc.cu).  E16/S16 rows are dp = d rounded up
+// to 8 16-bit elements.  Returns launches, or -1 if unsupported (tensor maps
+// or shared-memory budget).
+int tc_padded_width(uint64_t d);
+int tc_tile_n(uint32_t cap, uint64_t d);
+int launch_to16(const float* E32, uint64_t rows, uint64_t d, void* E16,
+                bool bf16, cudaStream_t st);
+int launch_cdist_tc(const void* E16, const void* S16, bool bf16,
+                    const float* E32, const float* nE, uint64_t V, uint64_t d,
+                    const SourceSel& s, float expo, float* K, float* KM, int ld,
+                    unsigned* err, int num_sms, cudaStream_t st);
 
 // Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
 // target document.  Returns launches issued (0 on unsupported vr_cap).
