@@ -54,6 +54,9 @@ def args_():
                     help="time budget of the CPU-baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cdist", choices=["fp32", "fp16", "bf16"], default="fp32",
+                    help="cost-panel precision: fp32 CUDA cores (plain form) or "
+                         "tcgen05 tensor cores with 16-bit operands")
     return ap.parse_args()
 
 
@@ -259,6 +262,7 @@ def ours(a, rank, world, local):
     W = WORKLOAD
 
     eng = wmd.Engine(local)
+    eng.set_cdist_mode(a.cdist)
     eng.set_embeddings(p.vecs)
     eng.set_targets(p.col_ptr, p.row_inds, p.vals)
     eng.set_timing(True)
@@ -283,7 +287,8 @@ def ours(a, rank, world, local):
                           p.max_iter)
     got = out[:sub].cpu().numpy()
     max_rel = float(np.max(np.abs(got - ref) / np.abs(ref)))
-    if not max_rel <= 1e-5:
+    tol = {"fp32": 1e-5, "fp16": 1e-4, "bf16": 1e-3}[a.cdist]
+    if not max_rel <= tol:
         raise SystemExit(f"bench: result check failed, max rel err {max_rel:.3e}")
 
     sampler = ClockSampler(local)
@@ -340,7 +345,10 @@ def ours(a, rank, world, local):
     peak_hbm, peak_src = measured_peaks()
     sm_mhz = clocks.get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-    dominant = "solve_kernel" if sv_ms >= cd_ms else "cdist_fp32_kernel"
+    cd_name = "cdist_fp32_kernel" if a.cdist == "fp32" else "cdist_tc_kernel"
+    if a.cdist != "fp32":
+        cdist_bytes = V * ((d + 7) // 8 * 8) * 2 + 2 * vr * V * 4
+    dominant = "solve_kernel" if sv_ms >= cd_ms else cd_name
     if dominant == "solve_kernel":
         ach = solve_bytes / (sv_ms * 1e-3) / 1e9
         fl = solve_flops / (sv_ms * 1e-3) / 1e12
@@ -403,9 +411,14 @@ def ours(a, rank, world, local):
             "ms_per_step": tot_ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "single-source plain Sinkhorn WMD "
-                                   "(FP32 cost panel + FP32 iterations, FP64 "
-                                   "final reduction)",
+            "config": {"workload": ("single-source plain Sinkhorn WMD (FP32 "
+                                    "cost panel + FP32 iterations, FP64 final "
+                                    "reduction)") if a.cdist == "fp32" else
+                                   (f"single-source Sinkhorn WMD, {a.cdist.upper()} "
+                                    "tensor-core cost panel with FP32 near-pair "
+                                    "recompute, FP32 iterations, FP64 final "
+                                    "reduction"),
+                       "cdist": a.cdist,
                        **WORKLOAD, "nnz_per_rank": p.nnz,
                        "docs_per_rank": p.N,
                        "l2": "flushed between steps (256 MiB write)",
