@@ -176,6 +176,45 @@ wmd_status wmd_stage_times(wmd_handle* h, float* select_ms, float* cdist_ms,
                            float* solve_ms);
 
 /* ---------------------------------------------------------------------------
+ * Allocation-free solve.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory: code running inside a
+ * framework or inference server that owns all device memory through its own
+ * pool and hands a plugin only its input and output buffers, or a
+ * latency-critical loop that cannot afford the device-wide synchronisation
+ * cudaMalloc / cudaFree imply.  This call allocates nothing (no cudaMalloc,
+ * cudaFree or allocating library routine); its working buffers live in a
+ * fixed 64 MiB scratch array compiled into the library, which every GPU that
+ * loads the library holds until the process exits.
+ *
+ * All pointers are DEVICE pointers on the current device: r_dev [V] (the
+ * dense source histogram), vecs_dev [V][d] FP32 row-major, 16-byte aligned,
+ * the target matrix as CSC (col_ptr_dev [N+1], row_inds_dev [nnz], vals_dev
+ * [nnz], the fields of wmd_csc_double_t) and the output wmd_dev [N].  vr_cap
+ * bounds the number of non-zeros of r (<= 1024).  lambda is the positive
+ * regulariser, K = exp(-lambda * M).  Runs the same kernels as the other
+ * entry points (FP32 cost panel) on `stream` (a cudaStream_t, NULL for the
+ * default stream) and returns after synchronising it.
+ *
+ * Limit: the problem must fit the scratch, 2*V*round_up(vr_cap,4)*4 + V*4 +
+ * nnz*8 + (N+1)*8 + vr_cap*(d+3)*4 bytes (plus small alignment padding)
+ * <= 64 MiB; larger problems return WMD_ERR_INVALID_ARG.
+ *
+ * The first call on each device resolves the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture begins.  Every call on a device shares the one
+ * scratch array, so calls that overlap on the GPU (other streams or host
+ * threads on the same device) race: serialise them.
+ */
+wmd_status wmd_sinkhorn_noalloc(const double* r_dev, const float* vecs_dev,
+                                uint64_t V, uint64_t d,
+                                const uint64_t* col_ptr_dev,
+                                const uint64_t* row_inds_dev,
+                                const double* vals_dev, uint64_t N,
+                                uint64_t nnz, uint64_t vr_cap, double lambda,
+                                int max_iter, double* wmd_dev, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Diagnostics.
  * ------------------------------------------------------------------------ */
 const char* wmd_status_string(wmd_status s);

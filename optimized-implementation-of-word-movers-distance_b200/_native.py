@@ -78,6 +78,10 @@ _SIGS = [
     ("wmd_set_timing", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_stage_times", ctypes.c_int,
      [ctypes.c_void_p, c_f32p, c_f32p, c_f32p]),
+    ("wmd_sinkhorn_noalloc", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, c_u64, ctypes.c_double,
+      ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     ("wmd_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("wmd_last_error", ctypes.c_char_p, []),
     ("wmd_abi_version", ctypes.c_int, []),

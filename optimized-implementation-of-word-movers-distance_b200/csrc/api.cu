@@ -75,6 +75,8 @@ std::string describe_err_bits(unsigned bits) {
 
 }  // namespace
 
+void wmd::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 struct wmd_handle {
   int device = 0;
   int sms = 0;

@@ -50,6 +50,9 @@ struct Targets {
   int64_t nnz = 0;
 };
 
+// Message returned by wmd_last_error() on the calling host thread.
+void set_last_error(const char* msg);
+
 inline int select_num_chunks(uint64_t V) {
   return (int)((V + kSelectChunk - 1) / kSelectChunk);
 }
