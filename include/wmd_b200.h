@@ -197,8 +197,9 @@ wmd_status wmd_stage_times(wmd_handle* h, float* select_ms, float* cdist_ms,
  * default stream) and returns after synchronising it.
  *
  * Limit: the problem must fit the scratch, 2*V*round_up(vr_cap,4)*4 + V*4 +
- * nnz*8 + (N+1)*8 + vr_cap*(d+3)*4 bytes (plus small alignment padding)
- * <= 64 MiB; larger problems return WMD_ERR_INVALID_ARG.
+ * nnz*8 + (N+1)*8 + vr_cap*(d+3)*4 bytes (plus about 33 KB of counters,
+ * near-pair list and alignment padding) <= 64 MiB; larger problems return
+ * WMD_ERR_INVALID_ARG.
  *
  * The first call on each device resolves the scratch array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call

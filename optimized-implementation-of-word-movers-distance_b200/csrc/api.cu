@@ -93,7 +93,7 @@ struct wmd_handle {
   bool have_T = false;
   // per query
   DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_S16, sel_vr, sel_chunks,
-      K, KM, out_dev, err_dev;
+      K, KM, out_dev, err_dev, near_pairs, near_count;
   unsigned* err_host = nullptr;      // pinned
   uint32_t* chunks_host = nullptr;   // pinned, grown with V
   size_t chunks_host_cap = 0;
@@ -284,7 +284,10 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   CK(h->sel_vr.ensure(sizeof(uint32_t)));
   CK(h->sel_chunks.ensure((size_t)nchunks * sizeof(uint32_t)));
   CK(h->K.ensure((size_t)V * ld * sizeof(float)));
-  CK(h->KM.ensure((size_t)V * ld * sizeof(float)));
+  // K.*M is stored only for expo = 0; otherwise the solve derives it from K.
+  const bool need_km = expo == 0.f;
+  if (need_km) CK(h->KM.ensure((size_t)V * ld * sizeof(float)));
+  float* KMp = need_km ? h->KM.as<float>() : nullptr;
   SourceSel sel;
   sel.ids = h->sel_ids.as<uint32_t>();
   sel.rinv = h->sel_rinv.as<float>();
@@ -316,16 +319,29 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     }
     CK(h->sel_S16.ensure((size_t)std::max<uint32_t>(cap, 1) * dp * 2));
   }
+  // Near-pair list for the exact fix-up of cancellation-prone entries.
+  const unsigned near_cap = (unsigned)std::min<uint64_t>(
+      (uint64_t)V * std::max<uint32_t>(cap, 1), 1u << 20);
+  CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
+  CK(h->near_count.ensure(sizeof(unsigned)));
+  NearList near;
+  near.pairs = h->near_pairs.as<uint2>();
+  near.count = h->near_count.as<unsigned>();
+  near.cap = near_cap;
+  near.E32 = h->E32.as<float>();
+  near.S32 = sel.S;
+  near.d = (int)d;
   if (h->timing) CK(cudaEventRecord(h->ev[0], h->stream));
   launches += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d,
                             sel, h->err_dev.as<unsigned>(), h->stream,
                             tcm ? h->E16.p : nullptr,
                             tcm ? h->sel_S16.p : nullptr, dp);
   if (h->timing) CK(cudaEventRecord(h->ev[1], h->stream));
+  CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
   if (tcm) {
     const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16, h->E32.as<float>(),
                                    h->nE.as<float>(), V, d, sel, expo,
-                                   h->K.as<float>(), h->KM.as<float>(), ld,
+                                   h->K.as<float>(), KMp, ld, near,
                                    h->err_dev.as<unsigned>(), h->sms, h->stream);
     if (lc < 0)
       return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable "
@@ -333,11 +349,14 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     launches += lc;
   } else {
     launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d,
-                                  sel, expo, h->K.as<float>(), h->KM.as<float>(),
-                                  ld, h->stream);
+                                  sel, expo, h->K.as<float>(), KMp, ld, near,
+                                  h->stream);
   }
+  launches += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
+                                h->nE.as<float>(), sel.nS, sel.vr, h->sms,
+                                h->stream);
   if (h->timing) CK(cudaEventRecord(h->ev[2], h->stream));
-  launches += launch_solve(h->K.as<float>(), h->KM.as<float>(), ld, cap, sel, t,
+  launches += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t,
                            max_iter, out_dev, h->stream);
   if (h->timing) CK(cudaEventRecord(h->ev[3], h->stream));
   CK(cudaGetLastError());
@@ -518,7 +537,8 @@ wmd_status wmd_destroy(wmd_handle* h) {
                     &h->ent, &h->order, &h->stage_cp, &h->stage_rows,
                     &h->stage_vals, &h->r_dev, &h->sel_ids, &h->sel_rinv,
                     &h->sel_S, &h->sel_nS, &h->sel_S16, &h->sel_vr,
-                    &h->sel_chunks, &h->K, &h->KM, &h->out_dev, &h->err_dev})
+                    &h->sel_chunks, &h->K, &h->KM, &h->out_dev, &h->err_dev,
+                    &h->near_pairs, &h->near_count})
     b->release();
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->chunks_host) cudaFreeHost(h->chunks_host);

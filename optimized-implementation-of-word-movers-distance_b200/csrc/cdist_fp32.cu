@@ -10,9 +10,11 @@
 // register-tiled SIMT GEMM over d).  That form cancels catastrophically for
 // close pairs (a word against itself gives M ~ 1e-3 instead of 0, i.e. a 1%
 // error in K at lambda = 10), so pairs whose GEMM-form M^2 falls below
-// max(0.25, (|E_w|^2 + |S_i|^2) / 30) are recomputed directly as
-// sqrt(sum_k (E_wk - S_ik)^2), the reference's formula (fused:35-43), in FP32.
-// Padding columns i >= v_r are written as K = KM = 0.
+// max(0.25, (|E_w|^2 + |S_i|^2) / 30) are listed for near_fixup_kernel, which
+// recomputes them directly as sqrt(sum_k (E_wk - S_ik)^2), the reference's
+// formula (fused:35-43), in FP32.
+// Padding columns i >= v_r are written as K = KM = 0.  KM is written only when
+// the caller passes a buffer for it (the solve needs it only for expo = 0).
 #include "wmd_internal.cuh"
 
 namespace wmd {
@@ -24,16 +26,6 @@ constexpr int BK = 16;         // d-slice per stage
 constexpr int THREADS = 128;   // 16 x 8 threads, each 8 rows x 4 sources
 constexpr int AS = BM + 4;     // padded smem row (floats)
 
-__device__ __forceinline__ float near_recompute(const float* __restrict__ a,
-                                                const float* __restrict__ b,
-                                                int d) {
-  float s = 0.f;
-  for (int k = 0; k < d; ++k) {
-    const float t = a[k] - b[k];
-    s = fmaf(t, t, s);
-  }
-  return s;
-}
 }  // namespace
 
 template <bool VEC4>
@@ -42,7 +34,8 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
                   uint64_t V, int d, const float* __restrict__ S,
                   const float* __restrict__ nS,
                   const uint32_t* __restrict__ vr_dev, float expo,
-                  float* __restrict__ Kout, float* __restrict__ KMout, int ld) {
+                  float* __restrict__ Kout, float* __restrict__ KMout, int ld,
+                  const NearList near) {
   __shared__ __align__(16) float As[2][BK][AS];
   __shared__ __align__(16) float Bs[2][BK][BN];
   const int tid = threadIdx.x;
@@ -144,25 +137,25 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
     }
   }
 
-  // Epilogue: M, recompute of near pairs, K = exp(expo*M), KM = K*M.
+  // Epilogue: M^2 from the GEMM form (near pairs listed for the exact
+  // fix-up pass), K = exp(expo*M), KM = K*M.
   const int c0 = n0 + tx * 4;
   if (c0 >= ld) return;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const uint64_t w = m0 + ty * 8 + i;
     if (w >= V) break;
-    float kv[4], kmv[4];
     const float ne = active ? nE[w] : 0.f;
+    float kv[4], kmv[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int c = c0 + j;
       kv[j] = 0.f;
       kmv[j] = 0.f;
+      const int c = c0 + j;
       if (c < vr) {
         const float ns = nS[c];
-        float m2 = fmaxf(ne + ns - 2.f * acc[i][j], 0.f);
-        if (m2 < fmaxf(0.25f, (ne + ns) * (1.f / 30.f)))
-          m2 = near_recompute(E + w * (uint64_t)d, S + (uint64_t)c * d, d);
+        const float m2 = fmaxf(ne + ns - 2.f * acc[i][j], 0.f);
+        if (m2 < near_threshold(ne, ns)) near_pair(near, w, c);
         const float m = sqrtf(m2);
         const float k = expf(expo * m);
         kv[j] = k;
@@ -171,21 +164,22 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
     }
     *reinterpret_cast<float4*>(Kout + w * (uint64_t)ld + c0) =
         make_float4(kv[0], kv[1], kv[2], kv[3]);
-    *reinterpret_cast<float4*>(KMout + w * (uint64_t)ld + c0) =
-        make_float4(kmv[0], kmv[1], kmv[2], kmv[3]);
+    if (KMout)
+      *reinterpret_cast<float4*>(KMout + w * (uint64_t)ld + c0) =
+          make_float4(kmv[0], kmv[1], kmv[2], kmv[3]);
   }
 }
 
 int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
                       const SourceSel& s, float expo, float* K, float* KM,
-                      int ld, cudaStream_t st) {
+                      int ld, const NearList& near, cudaStream_t st) {
   dim3 grid((unsigned)((V + BM - 1) / BM), (unsigned)((ld + BN - 1) / BN));
   if (d % 4 == 0)
     cdist_fp32_kernel<true><<<grid, THREADS, 0, st>>>(E32, nE, V, (int)d, s.S, s.nS,
-                                                      s.vr, expo, K, KM, ld);
+                                                      s.vr, expo, K, KM, ld, near);
   else
     cdist_fp32_kernel<false><<<grid, THREADS, 0, st>>>(E32, nE, V, (int)d, s.S, s.nS,
-                                                       s.vr, expo, K, KM, ld);
+                                                       s.vr, expo, K, KM, ld, near);
   return 1;
 }
 

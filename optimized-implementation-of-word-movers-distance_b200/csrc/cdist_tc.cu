@@ -13,11 +13,13 @@
 //               (M=128, N=NT, K=16) into a double-buffered FP32 accumulator
 //               and tcgen05.commit's stage-release / accumulator-ready
 //               barriers;
-//   warps 2-5   epilogue: tcgen05.ld of one accumulator row per thread,
+//   warps 2-9   epilogue: tcgen05.ld of one accumulator row per thread (two
+//               warps per TMEM lane quarter, splitting the columns),
 //               M^2 = |E_w|^2 + |S_i|^2 - 2 E_w.S_i with FP32 norms of the FP32
-//               embeddings, exact FP32 recompute sum_k (E_wk - S_ik)^2 of the
-//               pairs below max(0.25, (|E_w|^2+|S_i|^2)/30) (the cancellation-
-//               prone ones), then K = exp(expo*M), KM = K*M.
+//               embeddings, then K = exp(expo*M), KM = K*M.  Pairs below
+//               max(0.25, (|E_w|^2+|S_i|^2)/30) (the cancellation-prone ones)
+//               are appended to a list that near_fixup_kernel recomputes
+//               exactly afterwards, one warp per pair.
 //
 // Persistent grid: each CTA owns one N-tile of source words and walks the
 // vocabulary M-tiles blockIdx.x, blockIdx.x + gridDim.x, ...  No TMA
@@ -36,7 +38,7 @@ constexpr int BM = 128;          // vocabulary rows per tile (UMMA M)
 constexpr int BK = 64;           // 16-bit elements per 128-byte swizzle row
 constexpr int UK = 16;           // UMMA K per instruction
 constexpr int STAGES = 6;        // A-tile ring depth
-constexpr int kThreads = 192;    // 6 warps
+constexpr int kThreads = 320;    // 10 warps: producer, MMA, 8 epilogue
 constexpr int kTileBytesA = BM * BK * 2;  // 16 KB
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound per wait
 
@@ -154,7 +156,8 @@ struct Params {
   const float* nS;    // [cap]
   const uint32_t* vr; // device v_r
   float* K;           // [V][ld]
-  float* KM;          // [V][ld]
+  float* KM;          // [V][ld] or null (then K*M is not stored)
+  NearList near;      // cancellation-prone pairs for the exact fix-up pass
   unsigned* err;
   uint64_t V;
   int d, ld, NT, KT, tmem_cols;
@@ -202,7 +205,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
     mbar_init(bfull, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 4 * 32);
+      mbar_init(&acce[b], 8 * 32);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -274,18 +277,21 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
         }
       }
     } else {
-      // ---- epilogue: warps 2..5, one TMEM lane (= tile row) per thread ----
-      const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+      // ---- epilogue: warps 2..9.  A warp may only access its TMEM lane
+      // quarter (warp % 4); the two warps of a quarter split the columns in
+      // 16-column chunks.  One tile row per thread.
+      const int quarter = warp & 3;
+      const int half = (warp - 2) >> 2;
       const int row = quarter * 32 + lane;
       uint32_t t = 0;
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++t) {
         const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
-        if (!mbar_wait(&accf[b], tph, p.err)) break;
-        fence_after();
         const uint64_t w = (uint64_t)tile * BM + row;
         const bool wok = w < p.V;
-        const float ne = wok ? p.nE[w] : 0.f;
-        for (int c0 = 0; c0 < p.NT; c0 += 16) {
+        const float ne = wok ? p.nE[w] : 0.f;  // issued before the wait
+        if (!mbar_wait(&accf[b], tph, p.err)) break;
+        fence_after();
+        for (int c0 = 16 * half; c0 < p.NT; c0 += 32) {
           float acc[16];
           tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + b * p.NT + c0, acc);
           if (!wok) continue;
@@ -297,17 +303,8 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             kmv[j] = 0.f;
             if (i < vr) {
               const float ns = nS_s[c0 + j];
-              float m2 = fmaxf(ne + ns - 2.f * acc[j], 0.f);
-              if (m2 < fmaxf(0.25f, (ne + ns) * (1.f / 30.f))) {
-                const float* a = p.E32 + w * (uint64_t)p.d;
-                const float* s = p.S32 + (uint64_t)i * p.d;
-                float e = 0.f;
-                for (int k = 0; k < p.d; ++k) {
-                  const float dd = a[k] - s[k];
-                  e = fmaf(dd, dd, e);
-                }
-                m2 = e;
-              }
+              const float m2 = fmaxf(ne + ns - 2.f * acc[j], 0.f);
+              if (m2 < near_threshold(ne, ns)) near_pair(p.near, w, i);
               const float m = sqrtf(m2);
               const float kx = expf(p.expo * m);
               kv[j] = kx;
@@ -322,8 +319,9 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             if (c < p.ld) {
               *reinterpret_cast<float4*>(krow + c) = make_float4(
                   kv[4 * j4], kv[4 * j4 + 1], kv[4 * j4 + 2], kv[4 * j4 + 3]);
-              *reinterpret_cast<float4*>(kmrow + c) = make_float4(
-                  kmv[4 * j4], kmv[4 * j4 + 1], kmv[4 * j4 + 2], kmv[4 * j4 + 3]);
+              if (p.KM)
+                *reinterpret_cast<float4*>(kmrow + c) = make_float4(
+                    kmv[4 * j4], kmv[4 * j4 + 1], kmv[4 * j4 + 2], kmv[4 * j4 + 3]);
             }
           }
         }
@@ -331,7 +329,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
         mbar_arrive(&acce[b]);
       }
     }
-  } else if (warp >= 2) {
+  } else if (warp >= 2 && warp < 6) {
     // Pure padding tile (no source word in it): zero the panel columns.
     const int quarter = warp & 3;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -339,7 +337,8 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
       if (w >= p.V) continue;
       for (int c = n0; c < n0 + p.NT && c < p.ld; c += 4) {
         *reinterpret_cast<float4*>(p.K + w * (uint64_t)p.ld + c) = make_float4(0.f, 0.f, 0.f, 0.f);
-        *reinterpret_cast<float4*>(p.KM + w * (uint64_t)p.ld + c) = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p.KM)
+          *reinterpret_cast<float4*>(p.KM + w * (uint64_t)p.ld + c) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
   }
@@ -443,7 +442,8 @@ int launch_to16(const float* E32, uint64_t rows, uint64_t d, void* E16,
 int launch_cdist_tc(const void* E16, const void* S16, bool bf16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
-                    unsigned* err, int num_sms, cudaStream_t st) {
+                    const NearList& near, unsigned* err, int num_sms,
+                    cudaStream_t st) {
   const int dp = tc_padded_width(d);
   const int KT = (dp + tc::BK - 1) / tc::BK;
   const int NT = tc_tile_n(s.cap, d);
@@ -463,6 +463,7 @@ int launch_cdist_tc(const void* E16, const void* S16, bool bf16,
   p.vr = s.vr;
   p.K = K;
   p.KM = KM;
+  p.near = near;
   p.err = err;
   p.V = V;
   p.d = (int)d;

@@ -22,8 +22,8 @@
 // it.  Make that first call before any stream capture begins on the device.
 //
 // The kernels are the library's regular ones (norms, target packing and
-// validation, source selection, FP32 cost panel, fused solve); only where
-// their working buffers live differs.
+// validation, source selection, FP32 cost panel, near-pair fix-up, fused
+// solve); only where their working buffers live differs.
 #include <stdio.h>
 
 #include <mutex>
@@ -102,6 +102,9 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
   const size_t o_nE = off;     off += align256((size_t)V * 4);
   const size_t o_cp = off;     off += align256((size_t)(N + 1) * 8);
   const size_t o_ent = off;    off += align256((size_t)nnz * 8);
+  const unsigned near_cap = 4096;  // near-pair list (overflow -> panel scan)
+  const size_t o_ncnt = off;   off += align256(sizeof(unsigned));
+  const size_t o_npairs = off; off += align256((size_t)near_cap * 8);
   const size_t o_K = off;      off += align256((size_t)V * ld * 4);
   const size_t o_KM = off;     off += align256((size_t)V * ld * 4);
   if (off > kScratchBytes) {
@@ -137,24 +140,38 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
   float* K = reinterpret_cast<float*>(base + o_K);
   float* KM = reinterpret_cast<float*>(base + o_KM);
 
-  // The error word is the only scratch that must start at zero; every other
-  // region is fully written before it is read.
-  if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess) {
+  NearList near;
+  near.pairs = reinterpret_cast<uint2*>(base + o_npairs);
+  near.count = reinterpret_cast<unsigned*>(base + o_ncnt);
+  near.cap = near_cap;
+  near.E32 = vecs_dev;
+  near.S32 = sel.S;
+  near.d = (int)d;
+
+  // The error word and the near-pair counter are the only scratch that must
+  // start at zero; every other region is fully written before it is read.
+  if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess ||
+      cudaMemsetAsync(near.count, 0, sizeof(unsigned), st) != cudaSuccess) {
     cudaGetLastError();
-    return noalloc_fail(WMD_ERR_CUDA, "cudaMemsetAsync of the error word failed");
+    return noalloc_fail(WMD_ERR_CUDA, "cudaMemsetAsync of a scratch counter failed");
   }
   launch_embed_norms(vecs_dev, V, d, nE, st);
   launch_pack_targets(col_ptr_dev, row_inds_dev, vals_dev, V, N, nnz, cp, ent,
                       err, st);
   launch_select(r_dev, V, vecs_dev, nE, d, sel, err, st);
-  launch_cdist_fp32(vecs_dev, nE, V, d, sel, (float)(-lambda), K, KM, ld, st);
+  const float expo = (float)(-lambda);
+  float* KMp = expo == 0.f ? KM : nullptr;  // K.*M is needed only for lambda = 0
+  launch_cdist_fp32(vecs_dev, nE, V, d, sel, expo, K, KMp, ld, near, st);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  launch_near_fixup(near, expo, K, KMp, ld, V, nE, sel.nS, sel.vr, sms, st);
   Targets t;
   t.col_ptr = cp;
   t.ent = ent;
   t.order = nullptr;
   t.N = (int64_t)N;
   t.nnz = (int64_t)nnz;
-  launch_solve(K, KM, ld, cap, sel, t, max_iter, wmd_dev, st);
+  launch_solve(K, KMp, ld, expo, cap, sel, t, max_iter, wmd_dev, st);
 
   unsigned bits = 0;
   cudaError_t e = cudaMemcpyAsync(&bits, err, sizeof(unsigned),

@@ -4,7 +4,7 @@
 // Selection restates select_non_empty_entries (sinkhorn_wmd_fused.cpp:45-63):
 // every id with r != 0, in ascending id order, with weight r.  The reference
 // does it serially; here it is a two-launch stream compaction (count per
-// 4096-element chunk, then each chunk scans its flags and writes at the
+// 1024-element chunk, then each chunk scans its flags and writes at the
 // offset of the chunks before it), so the order is the reference's.
 #include "wmd_internal.cuh"
 

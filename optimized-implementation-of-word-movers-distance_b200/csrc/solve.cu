@@ -11,27 +11,50 @@
 //   s_k = K[w_k,:] . u,  v_k = c_k / s_k              (fused:339-366)
 //   WMD_j = sum_i u_i sum_k KM[w_k,i] v_k   (FP64)    (fused:367-393)
 //
+// The last line is evaluated as  WMD_j = sum_k v_k (KM[w_k,:] . u)  (the same
+// sum, regrouped by word, accumulated in FP64), and because K = exp(expo*M)
+// the K.*M entries are recovered from the K rows already on chip as
+// K ln(K) / expo; only expo = 0 (K = 1, M unrecoverable) reads a K.*M panel.
+//
 // A document's scalings depend only on its own column, so the whole loop runs
 // inside one warp with u and x in registers: no atomics (the reference needs
 // `omp atomic`, fused:284), no global u/x traffic and no per-iteration
-// launches.  The document's K rows (n x v_r, gathered from the L2-resident
-// panel) are staged once in shared memory and re-read from there by every
-// iteration; rows beyond the per-warp staging capacity are re-gathered from
-// L2.  KM rows are read once, by the final half-step.
+// launches.  The document's K rows are gathered once from the L2-resident
+// panel and re-used by every iteration from the fastest place they fit:
+// the first one or two rounds of rows stay in registers, the next ones are
+// staged in shared memory, any remainder is re-gathered from L2.  A
+// document's word ids and weights are staged first (independent loads), so
+// every row gather is issued from on-chip addresses without a dependent L2
+// round trip.
 //
-// Lane layout: LPW lanes share one word (a "group"), 32/LPW words are in
-// flight per warp step.  Lane q of a group owns DPL source dimensions, as the
-// float4 chunks q, q+LPW, q+2*LPW, ... of the row, so a group's lanes read
-// consecutive 16-byte chunks (one coalesced segment in L2, conflict-free in
-// shared memory; the two words of a 4-lane phase are separated by an XOR
-// swizzle of the staged row).
+// Lane layout: LPW lanes share one word and each owns 32 consecutive source
+// dimensions (lane q of the group: dimensions 32q..32q+31), so 32/LPW words
+// ("a round") are in flight per warp.  For v_r <= 32 (LPW = 1) each lane holds
+// a whole K row: the dot product K_w . u needs no shuffle and the 64 FMAs per
+// word run as 32 packed FFMA2.  The x accumulators of the word slots are
+// combined once per iteration through a swizzled 4 KB shared-memory
+// transpose, after which every lane recomputes u for its dimensions.
 #include "wmd_internal.cuh"
 
 namespace wmd {
 
+// Launch shape (warps per CTA, CTAs per SM) and arithmetic form: build-time
+// tuning knobs, the defaults being the measured best on B200.
+#ifndef WMD_SOLVE_WARPS
+#define WMD_SOLVE_WARPS 4
+#endif
+#ifndef WMD_SOLVE_CTAS_PER_SM
+#define WMD_SOLVE_CTAS_PER_SM 2
+#endif
+#ifndef WMD_SOLVE_PACKED_FMA
+#define WMD_SOLVE_PACKED_FMA 1
+#endif
+#ifndef WMD_SOLVE_REG_ROUNDS  // rounds of K rows kept in registers, LPW <= 4
+#define WMD_SOLVE_REG_ROUNDS 2
+#endif
+
 namespace {
-constexpr int kWarps = 8;                 // warps per CTA
-constexpr int kSmemBudget = 200 * 1024;   // dynamic shared memory per CTA
+constexpr int kWarps = WMD_SOLVE_WARPS;  // warps per CTA
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -41,229 +64,418 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+#if WMD_SOLVE_PACKED_FMA
+  return __ffma2_rn(a, b, c);
+#else
+  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+
+struct Row {  // one lane's 32-dimension slice of a K (or KM) row
+  float4 c[8];
+};
+
+__device__ __forceinline__ void zero_row(Row& r) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) r.c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
 }  // namespace
 
-template <int LPW, int DPL>
+template <int LPW>
 struct SolveShape {
-  static constexpr int WPS = 32 / LPW;  // words per warp step
-  static constexpr int RL = LPW * DPL;  // padded row length (floats)
+  static constexpr int WPS = 32 / LPW;  // words per round
+  static constexpr int RL = 32 * LPW;   // padded row length (floats)
   static constexpr int NCH = RL / 4;    // float4 chunks per padded row
-  static constexpr int CPL = DPL / 4;   // chunks per lane
-  static_assert(LPW >= 4 && LPW <= 32 && (LPW & (LPW - 1)) == 0, "LPW");
-  static_assert(DPL % 4 == 0, "DPL");
-  // Swizzle so the two words of an 8-lane shared-memory phase (LPW = 4) hit
-  // disjoint banks.  Wider groups already cover a full 128-byte phase.
-  static __device__ __forceinline__ int swz(int kk) {
-    return LPW == 4 ? ((kk & 1) << 2) : 0;
+  // Rounds of K rows kept in registers (fewer when the per-lane dimension
+  // arrays of wide sources already use the register budget).
+  static constexpr int RR = LPW <= 4 ? WMD_SOLVE_REG_ROUNDS : 1;
+  static_assert(LPW >= 1 && LPW <= 32 && (LPW & (LPW - 1)) == 0, "LPW");
+  // Per-warp shared memory: staged rows (whole rounds), staged entries
+  // {word id, weight} of the register and staged rounds, 32x32 transpose
+  // buffer, u broadcast buffer.  Every term is a multiple of 16 bytes.
+  static __host__ __device__ size_t entries_bytes(int srounds) {
+    return ((size_t)(srounds + RR) * WPS * 8 + 15) & ~(size_t)15;
+  }
+  static __host__ __device__ size_t warp_bytes(int srounds) {
+    return (size_t)srounds * WPS * RL * 4 + entries_bytes(srounds) +
+           32 * 32 * 4 + RL * 4;
   }
 };
 
-template <int LPW, int DPL>
-__global__ void __launch_bounds__(kWarps * 32)
+template <int LPW, bool FROM_KM>
+__global__ void __launch_bounds__(kWarps * 32, WMD_SOLVE_CTAS_PER_SM)
 solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
-             const uint32_t* __restrict__ vr_dev,
+             float expo, const uint32_t* __restrict__ vr_dev,
              const float* __restrict__ rinv,
              const int64_t* __restrict__ col_ptr,
              const uint2* __restrict__ ent,
              const int32_t* __restrict__ order, int64_t N, int max_iter,
-             int stage_rows, double* __restrict__ out) {
-  using Sh = SolveShape<LPW, DPL>;
+             int srounds, double* __restrict__ out) {
+  using Sh = SolveShape<LPW>;
+  constexpr int WPS = Sh::WPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = lane & (LPW - 1), g = lane / LPW;
-  float4* sK = reinterpret_cast<float4*>(smem_raw) +
-               (size_t)warp * stage_rows * Sh::NCH;
-  uint2* sE = reinterpret_cast<uint2*>(reinterpret_cast<float4*>(smem_raw) +
-                                       (size_t)kWarps * stage_rows * Sh::NCH) +
-              (size_t)warp * stage_rows;
+  const int srows = srounds * WPS;
+  unsigned char* wbase = smem_raw + (size_t)warp * Sh::warp_bytes(srounds);
+  float4* sK = reinterpret_cast<float4*>(wbase);
+  uint2* sE = reinterpret_cast<uint2*>(wbase + (size_t)srows * Sh::RL * 4);
+  float* red = reinterpret_cast<float*>(wbase + (size_t)srows * Sh::RL * 4 +
+                                        Sh::entries_bytes(srounds));
+  float* ubuf = red + 32 * 32;
   const int vr = (int)*vr_dev;
   const int ldc = ld >> 2;  // float4 chunks per global panel row
+  // Staged row s holds logical chunk 8q'+t at 8q' + (t ^ ((s*LPW + q') & 7)).
+  // For the lane that reads it s*LPW + q = 32*round + lane, so the key is
+  // lane & 7: constant per lane, and the 8 lanes of a shared-memory phase hit
+  // 8 distinct bank groups.
+  const int key = lane & 7;
 
-  // Per-lane constants: validity of each owned dimension and 1/r there.
-  static_assert(DPL <= 32, "validity mask is 32 bits");
-  float rv[DPL];
-  unsigned vmask = 0;
+  // Dimensions this lane finalises after the transpose: 32*qq + lane.
+  float rv[LPW];
+  unsigned dmask = 0;
 #pragma unroll
-  for (int t = 0; t < Sh::CPL; ++t)
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int i = 4 * (q + t * LPW) + e;
-      const bool ok = i < vr;
-      rv[t * 4 + e] = ok ? rinv[i] : 0.f;
-      vmask |= ok ? (1u << (t * 4 + e)) : 0u;
-    }
+  for (int qq = 0; qq < LPW; ++qq) {
+    const int D = 32 * qq + lane;
+    const bool ok = D < vr;
+    rv[qq] = ok ? rinv[D] : 0.f;
+    dmask |= ok ? (1u << qq) : 0u;
+  }
 
   const int64_t total_warps = (int64_t)gridDim.x * kWarps;
-  for (int64_t idx = (int64_t)blockIdx.x * kWarps + warp; idx < N;
-       idx += total_warps) {
-    const int64_t j = order ? (int64_t)order[idx] : idx;
-    const int64_t b = col_ptr[j];
-    const int n = (int)(col_ptr[j + 1] - b);
-    const int ns = n < stage_rows ? n : stage_rows;
+  int64_t idx = (int64_t)blockIdx.x * kWarps + warp;
+  // Pointers of the current document; the next one's are prefetched while
+  // this one is processed.
+  int64_t j = 0, b = 0;
+  int n = 0;
+  if (idx < N) {
+    j = order ? (int64_t)order[idx] : idx;
+    b = col_ptr[j];
+    n = (int)(col_ptr[j + 1] - b);
+  }
+  for (; idx < N; idx += total_warps) {
+    const int64_t nidx = idx + total_warps;
+    int64_t jn = 0;
+    if (nidx < N) jn = order ? (int64_t)__ldg(&order[nidx]) : nidx;
+    const int rounds = (n + WPS - 1) / WPS;
+    constexpr int RR = Sh::RR;
+    const int rr = rounds < RR ? rounds : RR;                   // in registers
+    const int sr = min(rounds - rr, srounds);                   // staged
+    const int lr = rounds - rr - sr;                            // from L2
+    const int ne = (rr + sr) * WPS;                             // staged entries
 
-    // Stage this document's entries and K rows [0, ns).
+    // Entries of the register and staged rounds (zero past the document).
     __syncwarp();
-    for (int k = lane; k < ns; k += 32) sE[k] = ent[b + k];
+#pragma unroll 4
+    for (int k = lane; k < ne; k += 32)
+      sE[k] = k < n ? __ldg(&ent[b + k]) : make_uint2(0u, 0u);
     __syncwarp();
-    for (int c = lane; c < ns * Sh::NCH; c += 32) {
-      const int kk = c / Sh::NCH, ch = c % Sh::NCH;
-      float4* dst = sK + kk * Sh::NCH + (ch ^ Sh::swz(kk));
-      if (ch < ldc)
-        cp_async16(dst, K + (size_t)sE[kk].x * ld + 4 * ch);
+    // Register rows: rounds [0, rr); zero rows and weights elsewhere.
+    Row reg[RR];
+    float creg[RR];
+#pragma unroll
+    for (int t = 0; t < RR; ++t) {
+      zero_row(reg[t]);
+      creg[t] = 0.f;
+      const int k = t * WPS + g;
+      if (t < rr && k < n) {
+        const uint2 en = sE[k];
+        creg[t] = __uint_as_float(en.y);
+        const float4* rp = reinterpret_cast<const float4*>(K + (size_t)en.x * ld);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (8 * q + c < ldc) reg[t].c[c] = __ldg(rp + 8 * q + c);
+      }
+    }
+    // Staged rows: rounds [rr, rr + sr), padded with zero rows to whole rounds.
+    for (int c = lane; c < sr * WPS * Sh::NCH; c += 32) {
+      const int s = c / Sh::NCH, lc = c % Sh::NCH;
+      const int k = rr * WPS + s;
+      float4* dst = sK + (size_t)s * Sh::NCH + 8 * (lc >> 3) +
+                    ((lc & 7) ^ ((s * LPW + (lc >> 3)) & 7));
+      if (k < n && lc < ldc)
+        cp_async16(dst, K + (size_t)sE[k].x * ld + 4 * lc);
       else
         *dst = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // Next document's pointers (the order[] load has landed by now).
+    int64_t bn = 0;
+    int nn = 0;
+    if (nidx < N) {
+      bn = __ldg(&col_ptr[jn]);
+      nn = (int)(__ldg(&col_ptr[jn + 1]) - bn);
     }
     cp_async_wait_all();
     __syncwarp();
 
-    // Row loader: staged rows from shared memory, the rest from L2.
-    auto load_row = [&](int kk, const float* __restrict__ P, bool use_stage,
-                        float (&kc)[DPL], float& cval) {
-      if (kk >= n) {
+    auto load_staged = [&](int s_round, Row& r, float& cval) {
+      const int s = s_round * WPS + g;
+      cval = __uint_as_float(sE[rr * WPS + s].y);
+      const float4* rp = sK + (size_t)s * Sh::NCH + 8 * q;
 #pragma unroll
-        for (int t = 0; t < DPL; ++t) kc[t] = 0.f;
-        cval = 0.f;
-        return;
-      }
-      if (use_stage && kk < ns) {
-        const uint2 en = sE[kk];
+      for (int t = 0; t < 8; ++t) r.c[t] = rp[t ^ key];
+    };
+    auto load_global = [&](const float* __restrict__ P, int k, Row& r,
+                           float& cval) {
+      zero_row(r);
+      cval = 0.f;
+      if (k < n) {
+        const uint2 en = __ldg(&ent[b + k]);
         cval = __uint_as_float(en.y);
+        const float4* rp = reinterpret_cast<const float4*>(P + (size_t)en.x * ld);
 #pragma unroll
-        for (int t = 0; t < Sh::CPL; ++t) {
-          const float4 v = sK[kk * Sh::NCH + ((q + t * LPW) ^ Sh::swz(kk))];
-          kc[4 * t + 0] = v.x; kc[4 * t + 1] = v.y;
-          kc[4 * t + 2] = v.z; kc[4 * t + 3] = v.w;
-        }
-      } else {
-        const uint2 en = kk < ns ? sE[kk] : __ldg(&ent[b + kk]);
-        cval = __uint_as_float(en.y);
-        const float* row = P + (size_t)en.x * ld;
-#pragma unroll
-        for (int t = 0; t < Sh::CPL; ++t) {
-          const int ch = q + t * LPW;
-          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (ch < ldc) v = __ldg(reinterpret_cast<const float4*>(row) + ch);
-          kc[4 * t + 0] = v.x; kc[4 * t + 1] = v.y;
-          kc[4 * t + 2] = v.z; kc[4 * t + 3] = v.w;
-        }
+        for (int t = 0; t < 8; ++t)
+          if (8 * q + t < ldc) r.c[t] = __ldg(rp + 8 * q + t);
       }
     };
-    auto group_sum = [&](float s) {
+    auto dot = [&](const Row& r, const float2 (&u2)[16]) {
+      float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        a0 = ffma2(make_float2(r.c[t].x, r.c[t].y), u2[2 * t], a0);
+        a1 = ffma2(make_float2(r.c[t].z, r.c[t].w), u2[2 * t + 1], a1);
+      }
+      float s = (a0.x + a1.x) + (a0.y + a1.y);
 #pragma unroll
       for (int off = 1; off < LPW; off <<= 1)
         s += __shfl_xor_sync(0xffffffffu, s, off);
       return s;
     };
-    auto cross_group_sum = [&](float (&x)[DPL]) {
+    auto axpy = [&](const Row& r, float v, float2 (&x2)[16]) {
+      const float2 vv = make_float2(v, v);
 #pragma unroll
-      for (int off = LPW; off < 32; off <<= 1)
+      for (int t = 0; t < 8; ++t) {
+        x2[2 * t] = ffma2(make_float2(r.c[t].x, r.c[t].y), vv, x2[2 * t]);
+        x2[2 * t + 1] = ffma2(make_float2(r.c[t].z, r.c[t].w), vv, x2[2 * t + 1]);
+      }
+    };
+    // v = c / s for a real word; exactly 0 for the padding words (c = 0 and
+    // a zero row), which would otherwise give 0/0.
+    auto weight = [](float c, float s) { return c != 0.f ? __fdividef(c, s) : 0.f; };
+    // Sum the x slices of all word slots: lane writes its 32 values as row
+    // `lane` of a 32x32 buffer (chunk-swizzled), then lane L sums column L for
+    // each of its LPW dimension groups: tot[qq] is dimension 32*qq + L.
+    auto reduce_slots = [&](const float2 (&x2)[16], float (&tot)[LPW]) {
+      float4* rw = reinterpret_cast<float4*>(red + lane * 32);
 #pragma unroll
-        for (int t = 0; t < DPL; ++t) x[t] += __shfl_xor_sync(0xffffffffu, x[t], off);
+      for (int t = 0; t < 8; ++t)
+        rw[t ^ key] = make_float4(x2[2 * t].x, x2[2 * t].y, x2[2 * t + 1].x,
+                                  x2[2 * t + 1].y);
+      __syncwarp();
+#pragma unroll
+      for (int qq = 0; qq < LPW; ++qq) {
+        float part[WPS];
+#pragma unroll
+        for (int gg = 0; gg < WPS; ++gg) {
+          const int row = gg * LPW + qq;
+          part[gg] = red[row * 32 + 4 * ((lane >> 2) ^ (row & 7)) + (lane & 3)];
+        }
+#pragma unroll
+        for (int w = WPS / 2; w >= 1; w >>= 1)
+#pragma unroll
+          for (int i = 0; i < w; ++i) part[i] += part[i + w];
+        tot[qq] = part[0];
+      }
+      __syncwarp();
+    };
+    auto broadcast_u = [&](const float (&uval)[LPW], float2 (&u2)[16]) {
+#pragma unroll
+      for (int qq = 0; qq < LPW; ++qq) ubuf[32 * qq + lane] = uval[qq];
+      __syncwarp();
+      const float4* ub = reinterpret_cast<const float4*>(ubuf + 32 * q);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const float4 v = ub[t];
+        u2[2 * t] = make_float2(v.x, v.y);
+        u2[2 * t + 1] = make_float2(v.z, v.w);
+      }
+      __syncwarp();
+    };
+    // One pass of v = c ./ (K^T u), x += K v over all rounds of the document.
+    auto pass = [&](const float2 (&u2)[16], float2 (&x2)[16]) {
+#pragma unroll
+      for (int t = 0; t < 16; ++t) x2[t] = make_float2(0.f, 0.f);
+      {
+        float sreg[RR];
+#pragma unroll
+        for (int t = 0; t < RR; ++t) sreg[t] = dot(reg[t], u2);
+#pragma unroll
+        for (int t = 0; t < RR; ++t) axpy(reg[t], weight(creg[t], sreg[t]), x2);
+      }
+      int t = 0;
+      for (; t + 1 < sr; t += 2) {
+        Row ra, rb;
+        float ca, cb;
+        load_staged(t, ra, ca);
+        load_staged(t + 1, rb, cb);
+        const float sa = dot(ra, u2), sb = dot(rb, u2);
+        axpy(ra, weight(ca, sa), x2);
+        axpy(rb, weight(cb, sb), x2);
+      }
+      if (t < sr) {
+        Row ra;
+        float ca;
+        load_staged(t, ra, ca);
+        axpy(ra, weight(ca, dot(ra, u2)), x2);
+      }
+      for (int l = 0; l < lr; ++l) {
+        Row ra;
+        float ca;
+        load_global(K, (rr + sr + l) * WPS + g, ra, ca);
+        axpy(ra, weight(ca, dot(ra, u2)), x2);
+      }
     };
 
-    float u[DPL], x[DPL];
+    float2 u2[16];
+    {
+      float uval[LPW];
 #pragma unroll
-    for (int t = 0; t < DPL; ++t) u[t] = ((vmask >> t) & 1u) ? (float)vr : 0.f;
+      for (int qq = 0; qq < LPW; ++qq) uval[qq] = ((dmask >> qq) & 1u) ? (float)vr : 0.f;
+      broadcast_u(uval, u2);
+    }
 
     for (int it = 0; it < max_iter; ++it) {
+      float2 x2[16];
+      pass(u2, x2);
+      float tot[LPW], uval[LPW];
+      reduce_slots(x2, tot);
 #pragma unroll
-      for (int t = 0; t < DPL; ++t) x[t] = 0.f;
-#pragma unroll 2
-      for (int k0 = 0; k0 < n; k0 += Sh::WPS) {
-        const int kk = k0 + g;
-        float kc[DPL], cval;
-        load_row(kk, K, true, kc, cval);
-        float s = 0.f;
-#pragma unroll
-        for (int t = 0; t < DPL; ++t) s = fmaf(kc[t], u[t], s);
-        s = group_sum(s);
-        const float v = kk < n ? cval / s : 0.f;
-#pragma unroll
-        for (int t = 0; t < DPL; ++t) x[t] = fmaf(kc[t], v, x[t]);
-      }
-      cross_group_sum(x);
-#pragma unroll
-      for (int t = 0; t < DPL; ++t)
-        u[t] = ((vmask >> t) & 1u) ? 1.f / (rv[t] * x[t]) : 0.f;
+      for (int qq = 0; qq < LPW; ++qq)
+        uval[qq] = ((dmask >> qq) & 1u) ? __frcp_rn(rv[qq] * tot[qq]) : 0.f;
+      broadcast_u(uval, u2);
     }
 
-    // Final half-step with K.*M, then the FP64 reduction (fused:339-393).
-#pragma unroll
-    for (int t = 0; t < DPL; ++t) x[t] = 0.f;
-    for (int k0 = 0; k0 < n; k0 += Sh::WPS) {
-      const int kk = k0 + g;
-      float kc[DPL], km[DPL], cval, cdup;
-      load_row(kk, K, true, kc, cval);
-      float s = 0.f;
-#pragma unroll
-      for (int t = 0; t < DPL; ++t) s = fmaf(kc[t], u[t], s);
-      s = group_sum(s);
-      const float v = kk < n ? cval / s : 0.f;
-      load_row(kk, KM, false, km, cdup);
-#pragma unroll
-      for (int t = 0; t < DPL; ++t) x[t] = fmaf(km[t], v, x[t]);
-    }
-    cross_group_sum(x);
+    // Final half-step (fused:339-393): WMD = sum_k v_k (KM_k . u), FP64 sum.
+    const float km_scale = FROM_KM ? 1.f : 0.69314718f / expo;  // ln 2 / expo
     double acc = 0.0;
+    for (int t = 0; t < rounds; ++t) {
+      Row rk;
+      float ck;
+      const int k = t * WPS + g;
+      if (t < rr) {
+        rk = reg[0];
+        ck = creg[0];
 #pragma unroll
-    for (int t = 0; t < DPL; ++t)
-      if ((vmask >> t) & 1u) acc += (double)u[t] * (double)x[t];
+        for (int i = 1; i < RR; ++i)
+          if (t == i) {
+            rk = reg[i];
+            ck = creg[i];
+          }
+      } else if (t < rr + sr) {
+        load_staged(t - rr, rk, ck);
+      } else {
+        load_global(K, k, rk, ck);
+      }
+      const float v = weight(ck, dot(rk, u2));
+      float tk;
+      if (FROM_KM) {
+        Row rm;
+        float cm;
+        load_global(KM, k, rm, cm);
+        tk = dot(rm, u2);
+      } else {
+        // KM_i = K_i M_i = K_i log2(K_i) ln2 / expo; K_i = 0 contributes 0.
+        float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int off = 1; off < LPW; off <<= 1)
-      acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        for (int c = 0; c < 8; ++c) {
+          const float4 kk = rk.c[c];
+          const float l0 = kk.x > 0.f ? __log2f(kk.x) : 0.f;
+          const float l1 = kk.y > 0.f ? __log2f(kk.y) : 0.f;
+          const float l2 = kk.z > 0.f ? __log2f(kk.z) : 0.f;
+          const float l3 = kk.w > 0.f ? __log2f(kk.w) : 0.f;
+          const float2 uk0 = make_float2(u2[2 * c].x * kk.x, u2[2 * c].y * kk.y);
+          const float2 uk1 = make_float2(u2[2 * c + 1].x * kk.z, u2[2 * c + 1].y * kk.w);
+          a = ffma2(uk0, make_float2(l0, l1), a);
+          a = ffma2(uk1, make_float2(l2, l3), a);
+        }
+        tk = a.x + a.y;
+#pragma unroll
+        for (int off = 1; off < LPW; off <<= 1)
+          tk += __shfl_xor_sync(0xffffffffu, tk, off);
+        tk *= km_scale;
+      }
+      if (q == 0 && k < n) acc += (double)v * (double)tk;
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    // The reference sums u_i x'_i over dimensions (fused:382-393): a
+    // non-finite u_i (x_i = 0, e.g. an empty document) meets x'_i = 0 there
+    // and makes the document NaN, which the regrouped sum above cannot see.
+    bool bad = false;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int d0 = 32 * q + 2 * t;
+      bad |= (d0 < vr && !isfinite(u2[t].x)) || (d0 + 1 < vr && !isfinite(u2[t].y));
+    }
+    if (__any_sync(0xffffffffu, bad)) acc = __longlong_as_double(0x7ff8000000000000ll);
+    if (vr == 0) acc = 0.0;  // no source word: an empty sum (fused:387)
     if (lane == 0) out[j] = acc;
+    j = jn;
+    b = bn;
+    n = nn;
   }
 }
 
-template <int LPW, int DPL>
-static int launch_solve_t(const float* K, const float* KM, int ld,
+template <int LPW, bool FROM_KM>
+static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
                           const SourceSel& s, const Targets& t, int max_iter,
                           double* out, cudaStream_t st) {
-  using Sh = SolveShape<LPW, DPL>;
-  const int per_row = Sh::RL * 4 + 8;
-  int stage_rows = kSmemBudget / kWarps / per_row;
-  const size_t smem = (size_t)kWarps * stage_rows * per_row;
-  // Per-device one-time set-up: opt in to the large shared-memory carve-out
-  // and size the persistent grid.
+  using Sh = SolveShape<LPW>;
   constexpr int kMaxDev = 64;
-  static int per_sm_cache[kMaxDev] = {0};
+  constexpr int kBlocksPerSm = WMD_SOLVE_CTAS_PER_SM;
+  constexpr size_t kSmemPerSm = 227 * 1024;
   static int sms_cache[kMaxDev] = {0};
+  static int srounds_cache[kMaxDev] = {0};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= kMaxDev) dev = 0;
-  if (per_sm_cache[dev] == 0) {
-    cudaFuncSetAttribute(solve_kernel<LPW, DPL>,
+  if (sms_cache[dev] == 0) {
+    const size_t per_warp = (kSmemPerSm / kBlocksPerSm - 1024) / kWarps;
+    const size_t fixed = Sh::warp_bytes(0);
+    const size_t per_round = (size_t)Sh::WPS * (Sh::RL * 4 + 4);
+    int sr = per_warp > fixed ? (int)((per_warp - fixed) / per_round) : 0;
+    while (sr > 0 && Sh::warp_bytes(sr) > per_warp) --sr;
+    cudaFuncSetAttribute(solve_kernel<LPW, FROM_KM>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kSmemBudget);
-    int sms = 0, per_sm = 0;
+                         (int)(kWarps * Sh::warp_bytes(sr)));
+    int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, solve_kernel<LPW, DPL>, kWarps * 32, smem);
     sms_cache[dev] = sms > 0 ? sms : 1;
-    per_sm_cache[dev] = per_sm > 0 ? per_sm : 1;
+    srounds_cache[dev] = sr;
   }
-  const int sms = sms_cache[dev], per_sm = per_sm_cache[dev];
+  const int sr = srounds_cache[dev];
+  const size_t smem = (size_t)kWarps * Sh::warp_bytes(sr);
   int64_t want = (t.N + kWarps - 1) / kWarps;
-  int64_t grid = (int64_t)sms * per_sm;
+  int64_t grid = (int64_t)sms_cache[dev] * kBlocksPerSm;
   if (grid > want) grid = want;
   if (grid < 1) grid = 1;
-  solve_kernel<LPW, DPL><<<(unsigned)grid, kWarps * 32, smem, st>>>(
-      K, KM, ld, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N, max_iter,
-      stage_rows, out);
+  solve_kernel<LPW, FROM_KM><<<(unsigned)grid, kWarps * 32, smem, st>>>(
+      K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N, max_iter,
+      sr, out);
   return 1;
 }
 
-int launch_solve(const float* K, const float* KM, int ld, uint32_t vr_cap,
-                 const SourceSel& s, const Targets& t, int max_iter,
-                 double* out, cudaStream_t st) {
-  if (t.N <= 0) return 0;
-  if (vr_cap <= 32) return launch_solve_t<4, 8>(K, KM, ld, s, t, max_iter, out, st);
-  if (vr_cap <= 64) return launch_solve_t<8, 8>(K, KM, ld, s, t, max_iter, out, st);
-  if (vr_cap <= 128) return launch_solve_t<16, 8>(K, KM, ld, s, t, max_iter, out, st);
-  if (vr_cap <= 256) return launch_solve_t<32, 8>(K, KM, ld, s, t, max_iter, out, st);
-  if (vr_cap <= 512) return launch_solve_t<32, 16>(K, KM, ld, s, t, max_iter, out, st);
-  if (vr_cap <= 1024) return launch_solve_t<32, 32>(K, KM, ld, s, t, max_iter, out, st);
+template <bool FROM_KM>
+static int dispatch_solve(const float* K, const float* KM, int ld, float expo,
+                          uint32_t vr_cap, const SourceSel& s, const Targets& t,
+                          int max_iter, double* out, cudaStream_t st) {
+  if (vr_cap <= 32) return launch_solve_t<1, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
+  if (vr_cap <= 64) return launch_solve_t<2, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
+  if (vr_cap <= 128) return launch_solve_t<4, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
+  if (vr_cap <= 256) return launch_solve_t<8, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
+  if (vr_cap <= 512) return launch_solve_t<16, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
+  if (vr_cap <= 1024) return launch_solve_t<32, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
   return -1;
+}
+
+int launch_solve(const float* K, const float* KM, int ld, float expo,
+                 uint32_t vr_cap, const SourceSel& s, const Targets& t,
+                 int max_iter, double* out, cudaStream_t st) {
+  if (t.N <= 0) return 0;
+  if (KM)
+    return dispatch_solve<true>(K, KM, ld, expo, vr_cap, s, t, max_iter, out, st);
+  return dispatch_solve<false>(K, KM, ld, expo, vr_cap, s, t, max_iter, out, st);
 }
 
 }  // namespace wmd

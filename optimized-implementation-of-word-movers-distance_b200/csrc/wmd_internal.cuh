@@ -7,7 +7,8 @@
 //   S     [cap][d]  float   embeddings of the selected source words
 //   nS    [cap]     float   their squared norms
 //   K     [V][ld]   float   exp(expo * M) for every (vocabulary word, source word)
-//   KM    [V][ld]   float   K * M (only read by the final half-step)
+//   KM    [V][ld]   float   K * M, only when expo = 0 (otherwise the solve
+//                           recovers K*M from K as K ln(K) / expo)
 //   col_ptr [N+1]   int64   target columns (documents)
 //   ent   [nnz]     uint2   {word id, float bits of the normalised count}
 // ld = number of source words rounded up to a multiple of 4, so that every
@@ -29,8 +30,48 @@ enum : unsigned {
 };
 
 constexpr int kSelectThreads = 256;
-constexpr int kSelectPerThread = 16;
+constexpr int kSelectPerThread = 4;
 constexpr int kSelectChunk = kSelectThreads * kSelectPerThread;
+
+// Near-pair threshold: pairs whose GEMM-form squared distance falls below
+// this are recomputed exactly (the GEMM form cancels for close pairs).
+__host__ __device__ __forceinline__ float near_threshold(float na, float nb) {
+  return fmaxf(0.25f, (na + nb) * (1.f / 30.f));
+}
+
+// Exact FP32 |a - b|^2 computed by a whole warp (lanes split the d
+// coordinates, shuffle-reduced); every lane gets the result.  Must be called
+// by all 32 lanes.
+__device__ __forceinline__ float warp_sqdist(const float* __restrict__ a,
+                                             const float* __restrict__ b,
+                                             int d, int lane) {
+  float s = 0.f;
+  for (int k = lane; k < d; k += 32) {
+    const float t = a[k] - b[k];
+    s = fmaf(t, t, s);
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  return s;
+}
+
+// Cancellation-prone (vocabulary word, source word) pairs found by a cost-panel
+// epilogue, recomputed exactly by near_fixup_kernel.  When more than `cap`
+// pairs turn up, that kernel scans the whole panel instead (correct, only
+// slower).
+struct NearList {
+  uint2* pairs = nullptr;     // [cap] {word id, source index}
+  unsigned* count = nullptr;  // must be zero before the cost panel runs
+  unsigned cap = 0;
+  const float* E32 = nullptr;
+  const float* S32 = nullptr;
+  int d = 0;
+};
+
+__device__ __forceinline__ void near_pair(const NearList& nl, uint64_t w, int i) {
+  const unsigned pos = atomicAdd(nl.count, 1u);
+  if (pos < nl.cap) nl.pairs[pos] = make_uint2((unsigned)w, (unsigned)i);
+}
 
 struct SourceSel {
   uint32_t* ids = nullptr;     // [cap]
@@ -80,11 +121,11 @@ int launch_select(const double* r, uint64_t V, const float* E32,
                   unsigned* err, cudaStream_t st, const void* E16 = nullptr,
                   void* S16 = nullptr, int dp = 0);
 
-// FP32 CUDA-core cost panel: K = exp(expo * M), KM = K * M, M from the GEMM
-// form with near pairs recomputed directly.
+// FP32 CUDA-core cost panel: K = exp(expo * M), and KM = K * M when KM is
+// not null; M from the GEMM form with near pairs recomputed directly.
 int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
                       const SourceSel& s, float expo, float* K, float* KM,
-                      int ld, cudaStream_t st);
+                      int ld, const NearList& near, cudaStream_t st);
 
 // Tensor-core cost panel (cdist_tc.cu).  E16/S16 rows are dp = d rounded up
 // to 8 16-bit elements.  Returns launches, or -1 if unsupported (tensor maps
@@ -96,12 +137,20 @@ int launch_to16(const float* E32, uint64_t rows, uint64_t d, void* E16,
 int launch_cdist_tc(const void* E16, const void* S16, bool bf16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
-                    unsigned* err, int num_sms, cudaStream_t st);
+                    const NearList& near, unsigned* err, int num_sms,
+                    cudaStream_t st);
+
+// Exact FP32 recompute of the listed near pairs (after either cost panel);
+// pairs beyond the list capacity are recomputed by a full-panel scan.
+int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
+                      int ld, uint64_t V, const float* nE, const float* nS,
+                      const uint32_t* vr, int num_sms, cudaStream_t st);
 
 // Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
 // target document.  Returns launches issued (0 on unsupported vr_cap).
-int launch_solve(const float* K, const float* KM, int ld, uint32_t vr_cap,
-                 const SourceSel& s, const Targets& t, int max_iter,
-                 double* out, cudaStream_t st);
+// KM may be null unless expo == 0.
+int launch_solve(const float* K, const float* KM, int ld, float expo,
+                 uint32_t vr_cap, const SourceSel& s, const Targets& t,
+                 int max_iter, double* out, cudaStream_t st);
 
 }  // namespace wmd

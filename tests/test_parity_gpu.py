@@ -176,3 +176,16 @@ def test_device_resident_query_matches_host_query(wmd, full):
     with pytest.raises(wmd.WMDError):
         eng.check()
     eng.close()
+
+
+@pytest.mark.parametrize("lam", [0.0, 0.5, -1.0])
+def test_lambda_edge_values_vs_oracle(wmd, synth, oracle_mod, lam):
+    """lambda = 0 (K = 1: the solve reads the stored K.*M panel instead of
+    recovering M from K) and the reference's shipped nonfused sign
+    (lambda = -1: K = exp(+M))."""
+    p = synth.case(1500, 300, 80, 24, 8, 60, 30, 210)
+    ref = oracle_mod.sinkhorn(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                              p.row_inds, p.vals, lam, 15, nthreads=1)
+    got = wmd.sinkhorn_wmd_csc(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                               p.row_inds, p.vals, -lam, 15, "fused")
+    _check(got, ref)
