@@ -156,6 +156,30 @@ wmd_status wmd_query_dense_device(wmd_handle* h, const double* r_dev,
                                   uint64_t vr_cap, double lambda, int max_iter,
                                   double* wmd_dev);
 
+/* Many source documents in one call (the batched serving form; no reference
+ * counterpart, the reference solves one source per run).  Source s has the
+ * words src_ids[src_ptr[s] .. src_ptr[s+1]) — strictly ascending ids < V, as
+ * the reference's selection yields them (sinkhorn_wmd_fused.cpp:45-63) — with
+ * weights src_w (> 0).  At most 1024 words per source.  wmd_out (host,
+ * num_sources x N row-major) receives every source's scores against the
+ * resident target set; iters_out (host, optional, same shape) the
+ * per-document iteration counts. */
+wmd_status wmd_query_batch(wmd_handle* h, const uint64_t* src_ptr,
+                           const uint64_t* src_ids, const double* src_w,
+                           uint64_t num_sources, double lambda, int max_iter,
+                           double* wmd_out, int* iters_out);
+
+/* Per-document convergence stopping.  tol = 0 (default): every document runs
+ * exactly max_iter x-updates, as the reference does (sinkhorn_wmd_fused.cpp:
+ * 246).  tol > 0: a document stops after the first update whose marginal
+ * residual sum_i |u_i (K v)_i - r_i| (with the scalings entering the update)
+ * is <= tol, max_iter becoming a cap.  No reference counterpart (the
+ * reference fixes the iteration count, main.py:11-12). */
+wmd_status wmd_set_tolerance(wmd_handle* h, double tol);
+
+/* Number of x-updates each document of the last query took (host, N). */
+wmd_status wmd_last_iterations(wmd_handle* h, int* iters);
+
 /* Synchronises the handle's stream and reports device-side validation
  * failures of the calls issued since the previous check. */
 wmd_status wmd_check(wmd_handle* h);

@@ -201,6 +201,38 @@ class Engine:
                                     _ptr(out, ctypes.c_double)))
         return out
 
+    def query_batch(self, sources, lam: float, max_iter: int,
+                    want_iters: bool = False):
+        """sources: list of dense histograms r (length V) or of (ids,
+        weights) pairs.  Returns a (len(sources), N) array of scores (and the
+        per-document iteration counts if want_iters)."""
+        ptr = [0]
+        ids, ws = [], []
+        for src in sources:
+            if isinstance(src, tuple):
+                i, w = np.asarray(src[0], np.uint64), np.asarray(src[1], np.float64)
+                order = np.argsort(i, kind="stable")
+                i, w = i[order], w[order]
+            else:
+                r = np.asarray(src, np.float64)
+                i = np.nonzero(r)[0].astype(np.uint64)
+                w = r[i.astype(np.int64)]
+            ids.append(i)
+            ws.append(w)
+            ptr.append(ptr[-1] + i.size)
+        ptr = np.asarray(ptr, np.uint64)
+        ids = np.ascontiguousarray(np.concatenate(ids) if ids else np.zeros(0), np.uint64)
+        ws = np.ascontiguousarray(np.concatenate(ws) if ws else np.zeros(0), np.float64)
+        S = len(sources)
+        out = np.empty((S, self.N), np.float64)
+        it = np.empty((S, self.N), np.int32) if want_iters else None
+        check(lib().wmd_query_batch(
+            self._h, _ptr(ptr, ctypes.c_uint64), _ptr(ids, ctypes.c_uint64),
+            _ptr(ws, ctypes.c_double), S, float(lam), int(max_iter),
+            _ptr(out, ctypes.c_double),
+            it.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if want_iters else None))
+        return (out, it) if want_iters else out
+
     def query_device(self, r_dev_ptr: int, vr_cap: int, lam: float,
                      max_iter: int, out_dev_ptr: int):
         """Asynchronous solve on device pointers (e.g. torch ``data_ptr()``)
@@ -211,6 +243,17 @@ class Engine:
 
     def check(self):
         check(lib().wmd_check(self._h))
+
+    def set_tolerance(self, tol: float):
+        """0: fixed max_iter updates (the reference); > 0: stop each document
+        once its marginal residual is <= tol (max_iter becomes a cap)."""
+        check(lib().wmd_set_tolerance(self._h, float(tol)))
+
+    def last_iterations(self) -> np.ndarray:
+        it = np.empty(self.N, np.int32)
+        check(lib().wmd_last_iterations(
+            self._h, it.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return it
 
     def set_timing(self, enable: bool = True):
         check(lib().wmd_set_timing(self._h, int(bool(enable))))

@@ -75,6 +75,12 @@ _SIGS = [
     ("wmd_check", ctypes.c_int, [ctypes.c_void_p]),
     ("wmd_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("wmd_last_launch_count", ctypes.c_int, [ctypes.c_void_p]),
+    ("wmd_query_batch", ctypes.c_int,
+     [ctypes.c_void_p, c_u64p, c_u64p, c_f64p, c_u64, ctypes.c_double,
+      ctypes.c_int, c_f64p, ctypes.POINTER(ctypes.c_int)]),
+    ("wmd_set_tolerance", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    ("wmd_last_iterations", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("wmd_set_timing", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_stage_times", ctypes.c_int,
      [ctypes.c_void_p, c_f32p, c_f32p, c_f32p]),

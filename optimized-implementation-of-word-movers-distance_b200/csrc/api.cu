@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -73,6 +74,29 @@ std::string describe_err_bits(unsigned bits) {
   return s;
 }
 
+// Everything a captured query graph depends on.
+struct QueryKey {
+  const void* r = nullptr;
+  const void* out = nullptr;
+  uint32_t cap = 0;
+  float expo = 0.f;
+  int max_iter = -1;
+  int mode = -1;
+  bool timing = false;
+  uint64_t epoch = 0;
+  float tol = 0.f;
+  const void* bufs[13] = {};  // every device buffer the graph reads or writes
+  bool operator==(const QueryKey& o) const {
+    if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
+          max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
+          epoch == o.epoch && tol == o.tol))
+      return false;
+    for (int i = 0; i < 13; ++i)
+      if (bufs[i] != o.bufs[i]) return false;
+    return true;
+  }
+};
+
 }  // namespace
 
 void wmd::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
@@ -93,7 +117,10 @@ struct wmd_handle {
   bool have_T = false;
   // per query
   DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_S16, sel_vr, sel_chunks,
-      K, KM, out_dev, err_dev, near_pairs, near_count;
+      K, KM, out_dev, err_dev, near_pairs, near_count, iters;
+  // batched queries
+  DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
+  float tol = 0.f;  // per-document convergence tolerance (0: fixed count)
   unsigned* err_host = nullptr;      // pinned
   uint32_t* chunks_host = nullptr;   // pinned, grown with V
   size_t chunks_host_cap = 0;
@@ -101,6 +128,13 @@ struct wmd_handle {
   // stage timing
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // CUDA-graph replay of device queries; graph_epoch changes whenever a
+  // buffer or setting a captured graph depends on changes.
+  bool use_graphs = true;
+  uint64_t graph_epoch = 0;
+  QueryKey seen_key, graph_key;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0;
 };
 
 namespace {
@@ -164,6 +198,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
   h->d = d;
   h->have_E = true;
   h->e16_fmt = -1;
+  h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
 }
@@ -233,6 +268,7 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   h->N = N;
   h->nnz = nnz;
   h->have_T = true;
+  h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
 }
@@ -324,6 +360,7 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
       (uint64_t)V * std::max<uint32_t>(cap, 1), 1u << 20);
   CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
   CK(h->near_count.ensure(sizeof(unsigned)));
+  CK(h->iters.ensure((size_t)std::max<uint64_t>(h->N, 1) * sizeof(int)));
   NearList near;
   near.pairs = h->near_pairs.as<uint2>();
   near.count = h->near_count.as<unsigned>();
@@ -331,36 +368,108 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   near.E32 = h->E32.as<float>();
   near.S32 = sel.S;
   near.d = (int)d;
-  if (h->timing) CK(cudaEventRecord(h->ev[0], h->stream));
-  launches += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d,
-                            sel, h->err_dev.as<unsigned>(), h->stream,
-                            tcm ? h->E16.p : nullptr,
-                            tcm ? h->sel_S16.p : nullptr, dp);
-  if (h->timing) CK(cudaEventRecord(h->ev[1], h->stream));
-  CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
-  if (tcm) {
-    const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16, h->E32.as<float>(),
-                                   h->nE.as<float>(), V, d, sel, expo,
-                                   h->K.as<float>(), KMp, ld, near,
-                                   h->err_dev.as<unsigned>(), h->sms, h->stream);
-    if (lc < 0)
-      return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable "
-                                       "(tensor map encoding failed)");
-    launches += lc;
-  } else {
-    launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d,
-                                  sel, expo, h->K.as<float>(), KMp, ld, near,
-                                  h->stream);
+  // Everything below is stream work only (no allocation, no host sync), so
+  // it can be captured into a CUDA graph and replayed.
+  auto record = [&](int i, bool capturing) -> cudaError_t {
+    if (!h->timing) return cudaSuccess;
+    return capturing ? cudaEventRecordWithFlags(h->ev[i], h->stream,
+                                                cudaEventRecordExternal)
+                     : cudaEventRecord(h->ev[i], h->stream);
+  };
+  auto enqueue = [&](bool capturing, int* nlaunch) -> wmd_status {
+    int n = 0;
+    CK(record(0, capturing));
+    n += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d, sel,
+                       h->err_dev.as<unsigned>(), h->stream,
+                       tcm ? h->E16.p : nullptr, tcm ? h->sel_S16.p : nullptr, dp);
+    CK(record(1, capturing));
+    CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
+    if (tcm) {
+      const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16,
+                                     h->E32.as<float>(), h->nE.as<float>(), V, d,
+                                     sel, expo, h->K.as<float>(), KMp, ld, near,
+                                     h->err_dev.as<unsigned>(), h->sms, h->stream);
+      if (lc < 0)
+        return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable "
+                                         "(tensor map encoding failed)");
+      n += lc;
+    } else {
+      n += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d, sel,
+                             expo, h->K.as<float>(), KMp, ld, near, h->stream);
+    }
+    n += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
+                           h->nE.as<float>(), sel.nS, sel.vr, h->sms, h->stream);
+    CK(record(2, capturing));
+    SolveCtl ctl;
+    ctl.max_iter = max_iter;
+    ctl.tol = h->tol;
+    ctl.iters = h->iters.as<int>();
+    n += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t, ctl,
+                      out_dev, h->stream);
+    CK(record(3, capturing));
+    CK(cudaGetLastError());
+    *nlaunch = n;
+    return WMD_OK;
+  };
+
+  // Graph replay: the first call with a configuration runs eagerly (it also
+  // warms per-device launch caches), the second is captured and
+  // instantiated, later ones replay the instantiated graph.
+  QueryKey key;
+  key.r = r_dev;
+  key.out = out_dev;
+  key.cap = cap;
+  key.expo = expo;
+  key.max_iter = max_iter;
+  key.mode = (int)h->mode;
+  key.timing = h->timing;
+  key.epoch = h->graph_epoch;
+  key.tol = h->tol;
+  {
+    const DevBuf* used[13] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+                              &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
+                              &h->near_pairs, &h->sel_chunks, &h->iters};
+    for (int i = 0; i < 13; ++i) key.bufs[i] = used[i]->p;
   }
-  launches += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
-                                h->nE.as<float>(), sel.nS, sel.vr, h->sms,
-                                h->stream);
-  if (h->timing) CK(cudaEventRecord(h->ev[2], h->stream));
-  launches += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t,
-                           max_iter, out_dev, h->stream);
-  if (h->timing) CK(cudaEventRecord(h->ev[3], h->stream));
-  CK(cudaGetLastError());
-  h->last_launches = launches;
+  if (!h->use_graphs) {
+    int n = 0;
+    wmd_status st = enqueue(false, &n);
+    h->last_launches = launches + n;
+    return st;
+  }
+  if (h->graph_exec && h->graph_key == key) {
+    CK(cudaGraphLaunch(h->graph_exec, h->stream));
+    h->last_launches = launches + h->graph_launches;
+    return WMD_OK;
+  }
+  if (!(h->seen_key == key)) {
+    h->seen_key = key;
+    int n = 0;
+    wmd_status st = enqueue(false, &n);
+    h->last_launches = launches + n;
+    return st;
+  }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int n = 0;
+  wmd_status st = enqueue(true, &n);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+  if (st != WMD_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  CK(ce);
+  const cudaError_t ie = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  CK(ie);
+  h->graph_key = key;
+  h->graph_launches = n;
+  CK(cudaGraphLaunch(h->graph_exec, h->stream));
+  h->last_launches = launches + n;
   return WMD_OK;
 }
 
@@ -406,6 +515,151 @@ wmd_status query_host(wmd_handle* h, const double* r, float expo, int max_iter,
   h->last_launches += lc;
   CK(cudaMemcpyAsync(wmd_out, h->out_dev.p, h->N * sizeof(double),
                      cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+// Many sparse source documents against the resident target set.  Source s
+// holds words src_ids[src_ptr[s] .. src_ptr[s+1]) (strictly ascending, < V)
+// with weights src_w (> 0): the reference's select order (fused:45-63)
+// already applied.  All sources are uploaded once; per source a gather, the
+// cost panel, the near-pair fix-up and the solve run back to back on the
+// handle's stream, re-using the single-source working buffers.
+wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
+                       const uint64_t* src_ids, const double* src_w, uint64_t S,
+                       float expo, int max_iter, double* wmd_out, int* iters_out) {
+  if (!h->have_E || !h->have_T)
+    return fail(WMD_ERR_INVALID_ARG, "embeddings and targets must be set first");
+  if (h->tV != h->V)
+    return fail(WMD_ERR_INVALID_ARG, "target rows != vocabulary size");
+  if (!src_ptr || S == 0 || !wmd_out) return fail(WMD_ERR_INVALID_ARG, "bad batch");
+  if (max_iter < 0) return fail(WMD_ERR_INVALID_ARG, "max_iter < 0");
+  if (src_ptr[0] != 0) return fail(WMD_ERR_INVALID_INPUT, "src_ptr[0] != 0");
+  const uint64_t total = src_ptr[S];
+  if (total && (!src_ids || !src_w)) return fail(WMD_ERR_INVALID_ARG, "null source arrays");
+  const uint64_t V = h->V, d = h->d, N = h->N;
+  std::vector<uint32_t> ids32(std::max<uint64_t>(total, 1));
+  std::vector<float> rinv(std::max<uint64_t>(total, 1));
+  std::vector<uint32_t> vrs(S);
+  uint32_t vr_max = 1;
+  for (uint64_t s = 0; s < S; ++s) {
+    if (src_ptr[s + 1] < src_ptr[s])
+      return fail(WMD_ERR_INVALID_INPUT, "source pointers decrease");
+    const uint64_t n = src_ptr[s + 1] - src_ptr[s];
+    if (n > 1024) return fail(WMD_ERR_UNSUPPORTED, "a source has more than 1024 words");
+    vrs[s] = (uint32_t)n;
+    vr_max = std::max<uint32_t>(vr_max, (uint32_t)n);
+    for (uint64_t e = src_ptr[s]; e < src_ptr[s + 1]; ++e) {
+      if (src_ids[e] >= V) return fail(WMD_ERR_INVALID_INPUT, "source word id >= V");
+      if (e > src_ptr[s] && src_ids[e] <= src_ids[e - 1])
+        return fail(WMD_ERR_INVALID_INPUT, "source word ids not strictly ascending");
+      if (!(src_w[e] > 0.0) || !std::isfinite(src_w[e]))
+        return fail(WMD_ERR_INVALID_INPUT, "source weight <= 0 or not finite");
+      ids32[e] = (uint32_t)src_ids[e];
+      rinv[e] = (float)(1.0 / src_w[e]);
+    }
+  }
+  const bool tcm = h->mode != WMD_CDIST_FP32;
+  const bool bf16 = h->mode == WMD_CDIST_BF16;
+  const int dp = tc_padded_width(d);
+  if (tcm && tc_tile_n(vr_max, d) == 0)
+    return fail(WMD_ERR_UNSUPPORTED, "embedding width too large for the tensor-core panel");
+  const int ld_max = (int)((vr_max + 3u) & ~3u);
+  CK(h->b_ids.ensure(ids32.size() * sizeof(uint32_t)));
+  CK(h->b_rinv.ensure(rinv.size() * sizeof(float)));
+  CK(h->b_vr.ensure(S * sizeof(uint32_t)));
+  CK(h->b_out.ensure(S * N * sizeof(double)));
+  CK(h->b_iters.ensure(S * N * sizeof(int)));
+  CK(h->sel_S.ensure((size_t)vr_max * d * sizeof(float)));
+  CK(h->sel_nS.ensure((size_t)vr_max * sizeof(float)));
+  CK(h->K.ensure((size_t)V * ld_max * sizeof(float)));
+  const bool need_km = expo == 0.f;
+  if (need_km) CK(h->KM.ensure((size_t)V * ld_max * sizeof(float)));
+  float* KMp = need_km ? h->KM.as<float>() : nullptr;
+  const unsigned near_cap = (unsigned)std::min<uint64_t>((uint64_t)V * vr_max, 1u << 20);
+  CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
+  CK(h->near_count.ensure(sizeof(unsigned)));
+  int launches = 0;
+  if (tcm) {
+    const int fmt = bf16 ? 1 : 2;
+    if (h->e16_fmt != fmt) {
+      CK(h->E16.ensure((size_t)V * dp * 2));
+      launches += launch_to16(h->E32.as<float>(), V, d, h->E16.p, bf16, h->stream);
+      h->e16_fmt = fmt;
+    }
+    CK(h->sel_S16.ensure((size_t)vr_max * dp * 2));
+  }
+  wmd_status st = clear_err(h);
+  if (st) return st;
+  CK(cudaMemcpyAsync(h->b_ids.p, ids32.data(), ids32.size() * sizeof(uint32_t),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->b_rinv.p, rinv.data(), rinv.size() * sizeof(float),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->b_vr.p, vrs.data(), S * sizeof(uint32_t),
+                     cudaMemcpyHostToDevice, h->stream));
+  Targets t;
+  t.col_ptr = h->col_ptr.as<int64_t>();
+  t.ent = h->ent.as<uint2>();
+  t.order = h->order.as<int32_t>();
+  t.N = (int64_t)N;
+  t.nnz = (int64_t)h->nnz;
+  if (h->timing)
+    for (int i = 0; i < 3; ++i) CK(cudaEventRecord(h->ev[i], h->stream));
+  for (uint64_t s = 0; s < S; ++s) {
+    const uint64_t off = src_ptr[s];
+    const uint32_t vr = vrs[s];
+    const int ld = (int)(((vr ? vr : 1) + 3u) & ~3u);
+    SourceSel sel;
+    sel.ids = h->b_ids.as<uint32_t>() + off;
+    sel.rinv = h->b_rinv.as<float>() + off;
+    sel.S = h->sel_S.as<float>();
+    sel.nS = h->sel_nS.as<float>();
+    sel.vr = h->b_vr.as<uint32_t>() + s;
+    sel.cap = vr;
+    NearList near;
+    near.pairs = h->near_pairs.as<uint2>();
+    near.count = h->near_count.as<unsigned>();
+    near.cap = near_cap;
+    near.E32 = h->E32.as<float>();
+    near.S32 = sel.S;
+    near.d = (int)d;
+    launches += launch_gather_sources(sel.ids, (int)vr, h->E32.as<float>(),
+                                      h->nE.as<float>(), d, sel.S, sel.nS,
+                                      tcm ? h->E16.p : nullptr,
+                                      tcm ? h->sel_S16.p : nullptr, dp, h->stream);
+    CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
+    if (tcm) {
+      const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16, h->E32.as<float>(),
+                                     h->nE.as<float>(), V, d, sel, expo,
+                                     h->K.as<float>(), KMp, ld, near,
+                                     h->err_dev.as<unsigned>(), h->sms, h->stream);
+      if (lc < 0)
+        return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable");
+      launches += lc;
+    } else {
+      launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d,
+                                    sel, expo, h->K.as<float>(), KMp, ld, near,
+                                    h->stream);
+    }
+    launches += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
+                                  h->nE.as<float>(), sel.nS, sel.vr, h->sms,
+                                  h->stream);
+    SolveCtl ctl;
+    ctl.max_iter = max_iter;
+    ctl.tol = h->tol;
+    ctl.iters = h->b_iters.as<int>() + s * N;
+    const int ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
+                                h->b_out.as<double>() + s * N, h->stream);
+    if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "a source has more than 1024 words");
+    launches += ls;
+  }
+  if (h->timing) CK(cudaEventRecord(h->ev[3], h->stream));
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(wmd_out, h->b_out.p, S * N * sizeof(double),
+                     cudaMemcpyDeviceToHost, h->stream));
+  if (iters_out)
+    CK(cudaMemcpyAsync(iters_out, h->b_iters.p, S * N * sizeof(int),
+                       cudaMemcpyDeviceToHost, h->stream));
+  h->last_launches = launches;
   return finish(h);
 }
 
@@ -538,10 +792,12 @@ wmd_status wmd_destroy(wmd_handle* h) {
                     &h->stage_vals, &h->r_dev, &h->sel_ids, &h->sel_rinv,
                     &h->sel_S, &h->sel_nS, &h->sel_S16, &h->sel_vr,
                     &h->sel_chunks, &h->K, &h->KM, &h->out_dev, &h->err_dev,
-                    &h->near_pairs, &h->near_count})
+                    &h->near_pairs, &h->near_count, &h->iters, &h->b_ids,
+                    &h->b_rinv, &h->b_vr, &h->b_out, &h->b_iters})
     b->release();
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->chunks_host) cudaFreeHost(h->chunks_host);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   for (int i = 0; i < 4; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -614,6 +870,17 @@ wmd_status wmd_query_dense_device(wmd_handle* h, const double* r_dev,
                       wmd_dev);
 }
 
+wmd_status wmd_query_batch(wmd_handle* h, const uint64_t* src_ptr,
+                           const uint64_t* src_ids, const double* src_w,
+                           uint64_t num_sources, double lambda, int max_iter,
+                           double* wmd_out, int* iters_out) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  wmd_status s = bind(h);
+  if (s) return s;
+  return query_batch(h, src_ptr, src_ids, src_w, num_sources, (float)(-lambda),
+                     max_iter, wmd_out, iters_out);
+}
+
 wmd_status wmd_check(wmd_handle* h) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
   wmd_status s = bind(h);
@@ -624,6 +891,24 @@ wmd_status wmd_check(wmd_handle* h) {
 void* wmd_stream(wmd_handle* h) { return h ? (void*)h->stream : nullptr; }
 
 int wmd_last_launch_count(wmd_handle* h) { return h ? h->last_launches : 0; }
+
+wmd_status wmd_set_tolerance(wmd_handle* h, double tol) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (!(tol >= 0.0)) return fail(WMD_ERR_INVALID_ARG, "tolerance must be >= 0");
+  h->tol = (float)tol;
+  return WMD_OK;
+}
+
+wmd_status wmd_last_iterations(wmd_handle* h, int* iters) {
+  if (!h || !iters) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  if (!h->have_T || !h->iters.p) return fail(WMD_ERR_INVALID_ARG, "no query has run");
+  wmd_status s = bind(h);
+  if (s) return s;
+  CK(cudaMemcpyAsync(iters, h->iters.p, h->N * sizeof(int), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return WMD_OK;
+}
 
 wmd_status wmd_set_timing(wmd_handle* h, int enable) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");

@@ -171,7 +171,9 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
   t.order = nullptr;
   t.N = (int64_t)N;
   t.nnz = (int64_t)nnz;
-  launch_solve(K, KMp, ld, expo, cap, sel, t, max_iter, wmd_dev, st);
+  SolveCtl ctl;
+  ctl.max_iter = max_iter;
+  launch_solve(K, KMp, ld, expo, cap, sel, t, ctl, wmd_dev, st);
 
   unsigned bits = 0;
   cudaError_t e = cudaMemcpyAsync(&bits, err, sizeof(unsigned),

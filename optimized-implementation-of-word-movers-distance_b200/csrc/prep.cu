@@ -263,3 +263,43 @@ int launch_select(const double* r, uint64_t V, const float* E32,
 }
 
 }  // namespace wmd
+
+namespace wmd {
+
+// Batched queries: gather the embedding rows of one source document whose
+// (ascending, validated) word ids were uploaded with the batch.  One warp per
+// source word; also its squared norm and, when S16 is given, its 16-bit row.
+__global__ void gather_sources_kernel(const uint32_t* __restrict__ ids, int count,
+                                      const float* __restrict__ E32,
+                                      const float* __restrict__ nE, uint64_t d,
+                                      float* __restrict__ S, float* __restrict__ nS,
+                                      const unsigned short* __restrict__ E16,
+                                      unsigned short* __restrict__ S16, int dp) {
+  const int w = (int)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= count) return;
+  const uint64_t id = ids[w];
+  const float* src = E32 + id * d;
+  float* dst = S + (uint64_t)w * d;
+  for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
+  if (lane == 0) nS[w] = nE[id];
+  if (S16) {
+    const unsigned short* s16 = E16 + id * (uint64_t)dp;
+    unsigned short* d16 = S16 + (uint64_t)w * dp;
+    for (int k = lane; k < dp; k += 32) d16[k] = s16[k];
+  }
+}
+
+int launch_gather_sources(const uint32_t* ids, int count, const float* E32,
+                          const float* nE, uint64_t d, float* S, float* nS,
+                          const void* E16, void* S16, int dp, cudaStream_t st) {
+  if (count <= 0) return 0;
+  const int threads = 256;
+  const int blocks = (count * 32 + threads - 1) / threads;
+  gather_sources_kernel<<<blocks, threads, 0, st>>>(
+      ids, count, E32, nE, d, S, nS, static_cast<const unsigned short*>(E16),
+      static_cast<unsigned short*>(S16), dp);
+  return 1;
+}
+
+}  // namespace wmd

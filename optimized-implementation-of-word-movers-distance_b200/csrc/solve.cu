@@ -52,6 +52,12 @@ namespace wmd {
 #ifndef WMD_SOLVE_REG_ROUNDS  // rounds of K rows kept in registers, LPW <= 4
 #define WMD_SOLVE_REG_ROUNDS 2
 #endif
+#ifndef WMD_SOLVE_UNROLL  // staged rounds in flight per step
+#define WMD_SOLVE_UNROLL 2
+#endif
+#ifndef WMD_SOLVE_DOT_CHAINS  // independent accumulators per dot product
+#define WMD_SOLVE_DOT_CHAINS 2
+#endif
 
 namespace {
 constexpr int kWarps = WMD_SOLVE_WARPS;  // warps per CTA
@@ -111,7 +117,8 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              const int64_t* __restrict__ col_ptr,
              const uint2* __restrict__ ent,
              const int32_t* __restrict__ order, int64_t N, int max_iter,
-             int srounds, double* __restrict__ out) {
+             float tol, int* __restrict__ iters_out, int srounds,
+             double* __restrict__ out) {
   using Sh = SolveShape<LPW>;
   constexpr int WPS = Sh::WPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,13 +140,14 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   const int key = lane & 7;
 
   // Dimensions this lane finalises after the transpose: 32*qq + lane.
-  float rv[LPW];
+  float rv[LPW], rw[LPW];  // 1/r_i and r_i
   unsigned dmask = 0;
 #pragma unroll
   for (int qq = 0; qq < LPW; ++qq) {
     const int D = 32 * qq + lane;
     const bool ok = D < vr;
     rv[qq] = ok ? rinv[D] : 0.f;
+    rw[qq] = ok ? __frcp_rn(rv[qq]) : 0.f;
     dmask |= ok ? (1u << qq) : 0u;
   }
 
@@ -230,13 +238,21 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       }
     };
     auto dot = [&](const Row& r, const float2 (&u2)[16]) {
-      float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
+      constexpr int NC = WMD_SOLVE_DOT_CHAINS;
+      float2 a[NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i) a[i] = make_float2(0.f, 0.f);
 #pragma unroll
       for (int t = 0; t < 8; ++t) {
-        a0 = ffma2(make_float2(r.c[t].x, r.c[t].y), u2[2 * t], a0);
-        a1 = ffma2(make_float2(r.c[t].z, r.c[t].w), u2[2 * t + 1], a1);
+        a[(2 * t) % NC] = ffma2(make_float2(r.c[t].x, r.c[t].y), u2[2 * t], a[(2 * t) % NC]);
+        a[(2 * t + 1) % NC] =
+            ffma2(make_float2(r.c[t].z, r.c[t].w), u2[2 * t + 1], a[(2 * t + 1) % NC]);
       }
-      float s = (a0.x + a1.x) + (a0.y + a1.y);
+#pragma unroll
+      for (int w = NC / 2; w >= 1; w >>= 1)
+#pragma unroll
+        for (int i = 0; i < w; ++i) a[i] = make_float2(a[i].x + a[i + w].x, a[i].y + a[i + w].y);
+      float s = a[0].x + a[0].y;
 #pragma unroll
       for (int off = 1; off < LPW; off <<= 1)
         s += __shfl_xor_sync(0xffffffffu, s, off);
@@ -303,17 +319,19 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
 #pragma unroll
         for (int t = 0; t < RR; ++t) axpy(reg[t], weight(creg[t], sreg[t]), x2);
       }
+      constexpr int U = WMD_SOLVE_UNROLL;
       int t = 0;
-      for (; t + 1 < sr; t += 2) {
-        Row ra, rb;
-        float ca, cb;
-        load_staged(t, ra, ca);
-        load_staged(t + 1, rb, cb);
-        const float sa = dot(ra, u2), sb = dot(rb, u2);
-        axpy(ra, weight(ca, sa), x2);
-        axpy(rb, weight(cb, sb), x2);
+      for (; t + U <= sr; t += U) {
+        Row ra[U];
+        float ca[U], sa[U];
+#pragma unroll
+        for (int i = 0; i < U; ++i) load_staged(t + i, ra[i], ca[i]);
+#pragma unroll
+        for (int i = 0; i < U; ++i) sa[i] = dot(ra[i], u2);
+#pragma unroll
+        for (int i = 0; i < U; ++i) axpy(ra[i], weight(ca[i], sa[i]), x2);
       }
-      if (t < sr) {
+      for (; t < sr; ++t) {
         Row ra;
         float ca;
         load_staged(t, ra, ca);
@@ -335,16 +353,31 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       broadcast_u(uval, u2);
     }
 
-    for (int it = 0; it < max_iter; ++it) {
+    int it = 0;
+    while (it < max_iter) {
       float2 x2[16];
       pass(u2, x2);
       float tot[LPW], uval[LPW];
       reduce_slots(x2, tot);
+      // Marginal residual |u_i (K v)_i - r_i| with the u entering this
+      // update (still in the broadcast buffer: each lane reads only the
+      // entries it wrote itself).
+      float res = 0.f;
 #pragma unroll
-      for (int qq = 0; qq < LPW; ++qq)
-        uval[qq] = ((dmask >> qq) & 1u) ? __frcp_rn(rv[qq] * tot[qq]) : 0.f;
+      for (int qq = 0; qq < LPW; ++qq) {
+        const bool ok = (dmask >> qq) & 1u;
+        if (tol > 0.f && ok) res += fabsf(ubuf[32 * qq + lane] * tot[qq] - rw[qq]);
+        uval[qq] = ok ? __frcp_rn(rv[qq] * tot[qq]) : 0.f;
+      }
       broadcast_u(uval, u2);
+      ++it;
+      if (tol > 0.f) {
+#pragma unroll
+        for (int off = 16; off; off >>= 1) res += __shfl_xor_sync(0xffffffffu, res, off);
+        if (res <= tol) break;
+      }
     }
+    if (iters_out && lane == 0) iters_out[j] = it;
 
     // Final half-step (fused:339-393): WMD = sum_k v_k (KM_k . u), FP64 sum.
     const float km_scale = FROM_KM ? 1.f : 0.69314718f / expo;  // ln 2 / expo
@@ -419,8 +452,8 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
 
 template <int LPW, bool FROM_KM>
 static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
-                          const SourceSel& s, const Targets& t, int max_iter,
-                          double* out, cudaStream_t st) {
+                          const SourceSel& s, const Targets& t,
+                          const SolveCtl& ctl, double* out, cudaStream_t st) {
   using Sh = SolveShape<LPW>;
   constexpr int kMaxDev = 64;
   constexpr int kBlocksPerSm = WMD_SOLVE_CTAS_PER_SM;
@@ -451,31 +484,31 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   if (grid > want) grid = want;
   if (grid < 1) grid = 1;
   solve_kernel<LPW, FROM_KM><<<(unsigned)grid, kWarps * 32, smem, st>>>(
-      K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N, max_iter,
-      sr, out);
+      K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
+      ctl.max_iter, ctl.tol, ctl.iters, sr, out);
   return 1;
 }
 
 template <bool FROM_KM>
 static int dispatch_solve(const float* K, const float* KM, int ld, float expo,
                           uint32_t vr_cap, const SourceSel& s, const Targets& t,
-                          int max_iter, double* out, cudaStream_t st) {
-  if (vr_cap <= 32) return launch_solve_t<1, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
-  if (vr_cap <= 64) return launch_solve_t<2, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
-  if (vr_cap <= 128) return launch_solve_t<4, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
-  if (vr_cap <= 256) return launch_solve_t<8, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
-  if (vr_cap <= 512) return launch_solve_t<16, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
-  if (vr_cap <= 1024) return launch_solve_t<32, FROM_KM>(K, KM, ld, expo, s, t, max_iter, out, st);
+                          const SolveCtl& c, double* out, cudaStream_t st) {
+  if (vr_cap <= 32) return launch_solve_t<1, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 64) return launch_solve_t<2, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 128) return launch_solve_t<4, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 256) return launch_solve_t<8, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 512) return launch_solve_t<16, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 1024) return launch_solve_t<32, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
   return -1;
 }
 
 int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
-                 int max_iter, double* out, cudaStream_t st) {
+                 const SolveCtl& ctl, double* out, cudaStream_t st) {
   if (t.N <= 0) return 0;
   if (KM)
-    return dispatch_solve<true>(K, KM, ld, expo, vr_cap, s, t, max_iter, out, st);
-  return dispatch_solve<false>(K, KM, ld, expo, vr_cap, s, t, max_iter, out, st);
+    return dispatch_solve<true>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
+  return dispatch_solve<false>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
 }
 
 }  // namespace wmd

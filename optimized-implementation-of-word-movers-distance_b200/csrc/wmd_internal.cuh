@@ -121,6 +121,11 @@ int launch_select(const double* r, uint64_t V, const float* E32,
                   unsigned* err, cudaStream_t st, const void* E16 = nullptr,
                   void* S16 = nullptr, int dp = 0);
 
+// Batched queries: gather the rows of one source from its uploaded ids.
+int launch_gather_sources(const uint32_t* ids, int count, const float* E32,
+                          const float* nE, uint64_t d, float* S, float* nS,
+                          const void* E16, void* S16, int dp, cudaStream_t st);
+
 // FP32 CUDA-core cost panel: K = exp(expo * M), and KM = K * M when KM is
 // not null; M from the GEMM form with near pairs recomputed directly.
 int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
@@ -146,11 +151,22 @@ int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
                       int ld, uint64_t V, const float* nE, const float* nS,
                       const uint32_t* vr, int num_sms, cudaStream_t st);
 
+// Iteration control of the solve.  tol <= 0: exactly max_iter x-updates, as
+// the reference (sinkhorn_wmd_fused.cpp:246).  tol > 0: a document stops
+// after the first update whose marginal residual sum_i |u_i (K v)_i - r_i|
+// (measured with the scalings entering that update) is <= tol, or after
+// max_iter updates.  iters (optional, [N]) receives each document's count.
+struct SolveCtl {
+  int max_iter = 15;
+  float tol = 0.f;
+  int* iters = nullptr;
+};
+
 // Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
-// target document.  Returns launches issued (0 on unsupported vr_cap).
+// target document.  Returns launches issued (-1 on unsupported vr_cap).
 // KM may be null unless expo == 0.
 int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
-                 int max_iter, double* out, cudaStream_t st);
+                 const SolveCtl& ctl, double* out, cudaStream_t st);
 
 }  // namespace wmd

@@ -1,0 +1,40 @@
+"""GPU: per-document convergence stopping (tolerance on the marginal
+residual) against the oracle's converged FP64 mode, which applies the same
+stopping rule (iterate until sum_i |u_i (K v)_i - r_i| <= tol, then form the
+WMD with the updated scalings)."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("tol", [1e-3, 1e-5])
+def test_converged_solve_matches_fp64_oracle(wmd, synth, oracle_mod, tol):
+    p = synth.case(4000, 300, 300, 32, 8, 200, 60, 300)
+    cap = 3000
+    ref, ref_it, ref_res, _ = oracle_mod.sinkhorn_converged(
+        p.r, p.vecs.astype(np.float64), p.col_ptr, p.row_inds, p.vals, p.lam,
+        tol=tol, max_iter_cap=cap)
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.set_tolerance(tol)
+    got = eng.query(p.r, p.lam, cap)
+    it = eng.last_iterations()
+    # Iteration counts agree except where FP32 rounding moves the residual
+    # across the threshold by one update.
+    assert np.mean(np.abs(it - ref_it) <= 1) >= 0.97
+    same = it == ref_it
+    assert rel_err(got[same], ref[same]).max() <= 2e-5
+    # Documents stopping one update apart still agree to the tolerance scale.
+    assert rel_err(got, ref).max() <= 50 * tol
+    # tol = 0 restores the fixed count of the reference
+    eng.set_tolerance(0.0)
+    fixed = eng.query(p.r, p.lam, 15)
+    assert np.all(eng.last_iterations() == 15)
+    ref15 = oracle_mod.sinkhorn(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                                p.row_inds, p.vals, p.lam, 15)
+    assert rel_err(fixed, ref15).max() <= 1e-5
+    eng.close()

@@ -189,3 +189,39 @@ def test_lambda_edge_values_vs_oracle(wmd, synth, oracle_mod, lam):
     got = wmd.sinkhorn_wmd_csc(p.r, p.vecs.astype(np.float64), p.col_ptr,
                                p.row_inds, p.vals, -lam, 15, "fused")
     _check(got, ref)
+
+
+def test_device_query_graph_replay(wmd, synth, oracle_mod):
+    """Repeated device queries are captured once into a CUDA graph and
+    replayed; a query that grows the working buffers in between, or a new
+    target set, must never replay a graph holding stale addresses."""
+    import torch
+    p = synth.case(3000, 300, 400, 32, 8, 200, 50, 220)
+    ref = oracle_mod.sinkhorn(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                              p.row_inds, p.vals, p.lam, p.max_iter)
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    r = torch.from_numpy(p.r).cuda()
+    outs = []
+    for cap in (32, 32, 32, 32, 200, 32, 32):
+        out = torch.full((p.N,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        eng.query_device(r.data_ptr(), cap, p.lam, p.max_iter, out.data_ptr())
+        eng.check()
+        outs.append(out.cpu().numpy())
+        del out
+    for o in outs:
+        _check(o, ref)
+    np.testing.assert_array_equal(outs[0], outs[3])  # eager == replayed
+    np.testing.assert_array_equal(outs[0], outs[6])
+    # new target set (half the documents): same engine, same pointers
+    half = p.N // 2
+    cp = p.col_ptr[:half + 1]
+    eng.set_targets(cp, p.row_inds[:cp[-1]], p.vals[:cp[-1]])
+    out = torch.empty(half, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        eng.query_device(r.data_ptr(), 32, p.lam, p.max_iter, out.data_ptr())
+        eng.check()
+        np.testing.assert_array_equal(out.cpu().numpy(), outs[0][:half])
+    eng.close()
