@@ -156,6 +156,21 @@ wmd_status wmd_query_dense_device(wmd_handle* h, const double* r_dev,
                                   uint64_t vr_cap, double lambda, int max_iter,
                                   double* wmd_dev);
 
+/* k nearest target documents (1 <= k <= 1024): the query of wmd_query_dense
+ * followed by a GPU ranking of its N scores — ascending WMD, ties broken by
+ * document index, NaN (empty documents) last, i.e. exactly
+ * numpy.argsort(scores, kind="stable")[:k].  idx_out / wmd_out: host, k.
+ * No reference counterpart (the reference writes the unsorted scores,
+ * main.py:140-143). */
+wmd_status wmd_query_topk(wmd_handle* h, const double* r, double lambda,
+                          int max_iter, uint32_t k, uint32_t* idx_out,
+                          double* wmd_out);
+
+/* The same ranking of any device-resident score vector (n <= 2^32 - 1),
+ * asynchronous on the handle's stream; idx_dev / val_dev: device, k. */
+wmd_status wmd_topk_device(wmd_handle* h, const double* scores_dev, uint64_t n,
+                           uint32_t k, uint32_t* idx_dev, double* val_dev);
+
 /* Many source documents in one call (the batched serving form; no reference
  * counterpart, the reference solves one source per run).  Source s has the
  * words src_ids[src_ptr[s] .. src_ptr[s+1]) — strictly ascending ids < V, as

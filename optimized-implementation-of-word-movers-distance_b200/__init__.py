@@ -201,6 +201,24 @@ class Engine:
                                     _ptr(out, ctypes.c_double)))
         return out
 
+    def query_topk(self, r, lam: float, max_iter: int, k: int):
+        """k nearest documents: (indices, scores), ascending WMD, ties by
+        index, NaN last (numpy.argsort(scores, kind='stable')[:k])."""
+        r = _f64(r)
+        idx = np.empty(k, np.uint32)
+        val = np.empty(k, np.float64)
+        check(lib().wmd_query_topk(
+            self._h, _ptr(r, ctypes.c_double), float(lam), int(max_iter), int(k),
+            idx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+            _ptr(val, ctypes.c_double)))
+        return idx, val
+
+    def topk_device(self, scores_dev_ptr: int, n: int, k: int, idx_dev_ptr: int,
+                    val_dev_ptr: int):
+        check(lib().wmd_topk_device(self._h, ctypes.c_void_p(scores_dev_ptr), n,
+                                    int(k), ctypes.c_void_p(idx_dev_ptr),
+                                    ctypes.c_void_p(val_dev_ptr)))
+
     def query_batch(self, sources, lam: float, max_iter: int,
                     want_iters: bool = False):
         """sources: list of dense histograms r (length V) or of (ids,

@@ -75,6 +75,12 @@ _SIGS = [
     ("wmd_check", ctypes.c_int, [ctypes.c_void_p]),
     ("wmd_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("wmd_last_launch_count", ctypes.c_int, [ctypes.c_void_p]),
+    ("wmd_query_topk", ctypes.c_int,
+     [ctypes.c_void_p, c_f64p, ctypes.c_double, ctypes.c_int, ctypes.c_uint32,
+      ctypes.POINTER(ctypes.c_uint32), c_f64p]),
+    ("wmd_topk_device", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, c_u64, ctypes.c_uint32, ctypes.c_void_p,
+      ctypes.c_void_p]),
     ("wmd_query_batch", ctypes.c_int,
      [ctypes.c_void_p, c_u64p, c_u64p, c_f64p, c_u64, ctypes.c_double,
       ctypes.c_int, c_f64p, ctypes.POINTER(ctypes.c_int)]),

@@ -120,6 +120,8 @@ struct wmd_handle {
       K, KM, out_dev, err_dev, near_pairs, near_count, iters;
   // batched queries
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
+  // top-k
+  DevBuf topk_scratch, topk_idx, topk_val;
   float tol = 0.f;  // per-document convergence tolerance (0: fixed count)
   unsigned* err_host = nullptr;      // pinned
   uint32_t* chunks_host = nullptr;   // pinned, grown with V
@@ -513,9 +515,23 @@ wmd_status query_host(wmd_handle* h, const double* r, float expo, int max_iter,
                    h->out_dev.as<double>());
   if (s) return s;
   h->last_launches += lc;
-  CK(cudaMemcpyAsync(wmd_out, h->out_dev.p, h->N * sizeof(double),
-                     cudaMemcpyDeviceToHost, h->stream));
+  if (wmd_out)
+    CK(cudaMemcpyAsync(wmd_out, h->out_dev.p, h->N * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
+}
+
+// k nearest documents of the scores in scores_dev (device, n): ascending WMD,
+// ties by document index, NaN last.  Asynchronous on the handle's stream.
+wmd_status topk_device(wmd_handle* h, const double* scores_dev, uint64_t n,
+                       uint32_t k, uint32_t* idx_dev, double* val_dev) {
+  if (k == 0 || k > 1024) return fail(WMD_ERR_INVALID_ARG, "k must be in [1, 1024]");
+  if (n == 0 || n > 0xFFFFFFFFull) return fail(WMD_ERR_INVALID_ARG, "bad score count");
+  CK(h->topk_scratch.ensure(topk_scratch_bytes(n, (int)k)));
+  h->last_launches = launch_topk(scores_dev, n, (int)k, h->topk_scratch.p, idx_dev,
+                                 val_dev, h->stream);
+  CK(cudaGetLastError());
+  return WMD_OK;
 }
 
 // Many sparse source documents against the resident target set.  Source s
@@ -793,7 +809,8 @@ wmd_status wmd_destroy(wmd_handle* h) {
                     &h->sel_S, &h->sel_nS, &h->sel_S16, &h->sel_vr,
                     &h->sel_chunks, &h->K, &h->KM, &h->out_dev, &h->err_dev,
                     &h->near_pairs, &h->near_count, &h->iters, &h->b_ids,
-                    &h->b_rinv, &h->b_vr, &h->b_out, &h->b_iters})
+                    &h->b_rinv, &h->b_vr, &h->b_out, &h->b_iters,
+                    &h->topk_scratch, &h->topk_idx, &h->topk_val})
     b->release();
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->chunks_host) cudaFreeHost(h->chunks_host);
@@ -879,6 +896,38 @@ wmd_status wmd_query_batch(wmd_handle* h, const uint64_t* src_ptr,
   if (s) return s;
   return query_batch(h, src_ptr, src_ids, src_w, num_sources, (float)(-lambda),
                      max_iter, wmd_out, iters_out);
+}
+
+wmd_status wmd_query_topk(wmd_handle* h, const double* r, double lambda,
+                          int max_iter, uint32_t k, uint32_t* idx_out,
+                          double* wmd_out) {
+  if (!h || !r || !idx_out || !wmd_out) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  wmd_status s = bind(h);
+  if (s) return s;
+  if (k == 0 || k > 1024) return fail(WMD_ERR_INVALID_ARG, "k must be in [1, 1024]");
+  s = query_host(h, r, (float)(-lambda), max_iter, nullptr);
+  if (s) return s;
+  const int lq = h->last_launches;
+  CK(h->topk_idx.ensure(k * sizeof(uint32_t)));
+  CK(h->topk_val.ensure(k * sizeof(double)));
+  s = topk_device(h, h->out_dev.as<double>(), h->N, k, h->topk_idx.as<uint32_t>(),
+                  h->topk_val.as<double>());
+  if (s) return s;
+  h->last_launches += lq;
+  CK(cudaMemcpyAsync(idx_out, h->topk_idx.p, k * sizeof(uint32_t),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(wmd_out, h->topk_val.p, k * sizeof(double),
+                     cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+wmd_status wmd_topk_device(wmd_handle* h, const double* scores_dev, uint64_t n,
+                           uint32_t k, uint32_t* idx_dev, double* val_dev) {
+  if (!h || !scores_dev || !idx_dev || !val_dev)
+    return fail(WMD_ERR_INVALID_ARG, "null argument");
+  wmd_status s = bind(h);
+  if (s) return s;
+  return topk_device(h, scores_dev, n, k, idx_dev, val_dev);
 }
 
 wmd_status wmd_check(wmd_handle* h) {

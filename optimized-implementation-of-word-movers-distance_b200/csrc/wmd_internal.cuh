@@ -121,6 +121,12 @@ int launch_select(const double* r, uint64_t V, const float* E32,
                   unsigned* err, cudaStream_t st, const void* E16 = nullptr,
                   void* S16 = nullptr, int dp = 0);
 
+// Top-k nearest documents (topk.cu): stable ascending order of the FP64
+// scores, ties by index, NaN last.  1 <= k <= 1024.
+size_t topk_scratch_bytes(uint64_t n, int k);
+int launch_topk(const double* scores, uint64_t n, int k, void* scratch,
+                uint32_t* out_idx, double* out_val, cudaStream_t st);
+
 // Batched queries: gather the rows of one source from its uploaded ids.
 int launch_gather_sources(const uint32_t* ids, int count, const float* E32,
                           const float* nE, uint64_t d, float* S, float* nS,
