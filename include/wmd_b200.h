@@ -142,6 +142,18 @@ wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* c);
 
 wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode);
 
+/* Storage of the K panel the Sinkhorn iterations read.  FP32 (default) is
+ * the form held to 1e-5 against the reference.  BF16 applies to sources with
+ * 64 < v_r <= 512 and lambda != 0: the panel is rounded to BF16 and solved by
+ * the CTA-per-document kernel that keeps each document's rows in shared
+ * memory (iterations still in FP32, final reduction in FP64).  Other sources
+ * use the FP32 path in either setting. */
+typedef enum wmd_solve_precision {
+  WMD_SOLVE_FP32 = 0,
+  WMD_SOLVE_BF16 = 1
+} wmd_solve_precision;
+wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec);
+
 /* One source document as a dense host histogram r[V] (the reference's form,
  * zeros skipped as sinkhorn_wmd_fused.cpp:45-63 does).  wmd_out: host, N. */
 wmd_status wmd_query_dense(wmd_handle* h, const double* r, double lambda,

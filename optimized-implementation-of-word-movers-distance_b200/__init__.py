@@ -193,6 +193,11 @@ class Engine:
     def set_cdist_mode(self, mode: str):
         check(lib().wmd_set_cdist_mode(self._h, CDIST_MODES[mode]))
 
+    def set_solve_precision(self, prec: str):
+        """'fp32' (default) or 'bf16': K panel storage read by the iterations
+        for sources with 64 < v_r <= 512."""
+        check(lib().wmd_set_solve_precision(self._h, {"fp32": 0, "bf16": 1}[prec]))
+
     def query(self, r, lam: float, max_iter: int) -> np.ndarray:
         r = _f64(r)
         out = np.empty(self.N, np.float64)

@@ -67,6 +67,7 @@ _SIGS = [
     ("wmd_set_targets_csc", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSC)]),
     ("wmd_set_targets_csr", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSR)]),
     ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_set_solve_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_query_dense", ctypes.c_int,
      [ctypes.c_void_p, c_f64p, ctypes.c_double, ctypes.c_int, c_f64p]),
     ("wmd_query_dense_device", ctypes.c_int,

@@ -85,13 +85,14 @@ struct QueryKey {
   bool timing = false;
   uint64_t epoch = 0;
   float tol = 0.f;
-  const void* bufs[13] = {};  // every device buffer the graph reads or writes
+  int prec = -1;
+  const void* bufs[14] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
-          epoch == o.epoch && tol == o.tol))
+          epoch == o.epoch && tol == o.tol && prec == o.prec))
       return false;
-    for (int i = 0; i < 13; ++i)
+    for (int i = 0; i < 14; ++i)
       if (bufs[i] != o.bufs[i]) return false;
     return true;
   }
@@ -106,6 +107,9 @@ struct wmd_handle {
   int sms = 0;
   cudaStream_t stream = nullptr;
   wmd_cdist_mode mode = WMD_CDIST_FP32;
+  // Storage of the K panel the solve reads for 64 < v_r <= 512 (BF16: the
+  // CTA-per-document kernel with the rows staged in shared memory).
+  wmd_solve_precision prec = WMD_SOLVE_FP32;
   // embeddings
   DevBuf E32, nE, E64_stage, E16;
   uint64_t V = 0, d = 0;
@@ -117,7 +121,7 @@ struct wmd_handle {
   bool have_T = false;
   // per query
   DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_S16, sel_vr, sel_chunks,
-      K, KM, out_dev, err_dev, near_pairs, near_count, iters;
+      K, KM, K16, out_dev, err_dev, near_pairs, near_count, iters;
   // batched queries
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
   // top-k
@@ -326,6 +330,8 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   const bool need_km = expo == 0.f;
   if (need_km) CK(h->KM.ensure((size_t)V * ld * sizeof(float)));
   float* KMp = need_km ? h->KM.as<float>() : nullptr;
+  const int ld16 = h->prec == WMD_SOLVE_BF16 && !need_km ? block_panel_width(cap) : 0;
+  if (ld16) CK(h->K16.ensure((size_t)V * ld16 * 2));
   SourceSel sel;
   sel.ids = h->sel_ids.as<uint32_t>();
   sel.rinv = h->sel_rinv.as<float>();
@@ -406,8 +412,17 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->iters.as<int>();
-    n += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t, ctl,
-                      out_dev, h->stream);
+    if (ld16) {
+      n += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V, sel.vr,
+                                h->sms, h->stream);
+      const int ls = launch_solve_block(h->K16.p, ld16, expo, cap, sel, t, ctl,
+                                        nullptr, 0, out_dev, h->stream);
+      if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "block solve unavailable");
+      n += ls;
+    } else {
+      n += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t, ctl,
+                        out_dev, h->stream);
+    }
     CK(record(3, capturing));
     CK(cudaGetLastError());
     *nlaunch = n;
@@ -427,11 +442,12 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.timing = h->timing;
   key.epoch = h->graph_epoch;
   key.tol = h->tol;
+  key.prec = (int)h->prec;
   {
-    const DevBuf* used[13] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+    const DevBuf* used[14] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
                               &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
-                              &h->near_pairs, &h->sel_chunks, &h->iters};
-    for (int i = 0; i < 13; ++i) key.bufs[i] = used[i]->p;
+                              &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16};
+    for (int i = 0; i < 14; ++i) key.bufs[i] = used[i]->p;
   }
   if (!h->use_graphs) {
     int n = 0;
@@ -591,6 +607,10 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   const bool need_km = expo == 0.f;
   if (need_km) CK(h->KM.ensure((size_t)V * ld_max * sizeof(float)));
   float* KMp = need_km ? h->KM.as<float>() : nullptr;
+  int ld16_max = 0;
+  if (h->prec == WMD_SOLVE_BF16 && !need_km)
+    for (uint64_t s = 0; s < S; ++s) ld16_max = std::max(ld16_max, block_panel_width(vrs[s]));
+  if (ld16_max) CK(h->K16.ensure((size_t)V * ld16_max * 2));
   const unsigned near_cap = (unsigned)std::min<uint64_t>((uint64_t)V * vr_max, 1u << 20);
   CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
   CK(h->near_count.ensure(sizeof(unsigned)));
@@ -663,8 +683,17 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->b_iters.as<int>() + s * N;
-    const int ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
-                                h->b_out.as<double>() + s * N, h->stream);
+    const int ld16 = h->prec == WMD_SOLVE_BF16 && !KMp ? block_panel_width(vr) : 0;
+    int ls;
+    if (ld16) {
+      launches += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V,
+                                       sel.vr, h->sms, h->stream);
+      ls = launch_solve_block(h->K16.p, ld16, expo, vr, sel, t, ctl, nullptr, 0,
+                              h->b_out.as<double>() + s * N, h->stream);
+    } else {
+      ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
+                        h->b_out.as<double>() + s * N, h->stream);
+    }
     if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "a source has more than 1024 words");
     launches += ls;
   }
@@ -859,6 +888,14 @@ wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
   if (mode != WMD_CDIST_FP32 && mode != WMD_CDIST_BF16 && mode != WMD_CDIST_FP16)
     return fail(WMD_ERR_INVALID_ARG, "unknown cdist mode");
   h->mode = mode;
+  return WMD_OK;
+}
+
+wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (prec != WMD_SOLVE_FP32 && prec != WMD_SOLVE_BF16)
+    return fail(WMD_ERR_INVALID_ARG, "unknown solve precision");
+  h->prec = prec;
   return WMD_OK;
 }
 

@@ -175,4 +175,14 @@ int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
                  const SolveCtl& ctl, double* out, cudaStream_t st);
 
+// Wide-source solve (solve_block.cu): one CTA per document over a BF16 panel
+// [V][ld16], ld16 = block_panel_width(v_r) (0: not applicable).  u0, when
+// not null, is an initial scaling [N][ldu] (warm start, cold fallback).
+int block_panel_width(uint32_t vr_cap);
+int launch_panel_to_bf16(const float* K, int ld, void* K16, int ld16, uint64_t V,
+                         const uint32_t* vr, int num_sms, cudaStream_t st);
+int launch_solve_block(const void* K16, int ld16, float expo, uint32_t vr_cap,
+                       const SourceSel& s, const Targets& t, const SolveCtl& ctl,
+                       const float* u0, int64_t ldu, double* out, cudaStream_t st);
+
 }  // namespace wmd
