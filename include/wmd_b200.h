@@ -274,6 +274,61 @@ const char* wmd_status_string(wmd_status s);
 const char* wmd_last_error(void);
 int wmd_abi_version(void);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start.  No reference counterpart (the reference always starts
+ * from u = v_r, sinkhorn_wmd_fused.cpp:188-191).  A 3-layer MLP (256 GELU,
+ * 256 GELU, 1) predicts log u_i per (source word i, target document) from
+ * the source word's embedding, r_i, log r_i, the document's weighted
+ * embedding centroid and min / mean / max of M(i, w) over the document's
+ * words; queries then start from exp(prediction), and each document falls
+ * back to the cold start when the prediction's first-update marginal
+ * residual is worse.  Parameters are one FP32 vector of
+ * wmd_ws_param_count(d) floats: shift[F], scale[F], W1[256][F], b1[256],
+ * W2[256][256], b2[256], w3[256], b3 (+3 pad), F = 2d + 5 rounded up to 16.
+ * ------------------------------------------------------------------------ */
+uint64_t wmd_ws_param_count(uint64_t d);
+/* Seeded initial parameters (shift 0, scale 1, W ~ N(0, 1/fan_in), b = 0). */
+wmd_status wmd_ws_init_params(uint64_t d, uint64_t seed, float* params);
+/* Labels: for each source (same form as wmd_query_batch), `docs_per_source`
+ * documents of the handle's target set are drawn (seeded, without
+ * replacement) and solved to convergence in FP64 (marginal residual <=
+ * label_tol within label_max_iter updates); for each converged pair
+ * min(words_per_doc, v_r) source words become training rows (features,
+ * log u).  The rows stay on the GPU, standardised, for wmd_ws_train. */
+wmd_status wmd_ws_build_training_set(wmd_handle* h, const uint64_t* src_ptr,
+                                     const uint64_t* src_ids, const double* src_w,
+                                     uint64_t num_sources, double lambda,
+                                     uint32_t docs_per_source, uint32_t words_per_doc,
+                                     double label_tol, int label_max_iter,
+                                     uint64_t seed, uint64_t* rows_out,
+                                     uint64_t* groups_out, double* mean_label_iters);
+/* Adam on the group-centred squared error of log u (each (source, document)
+ * pair's mean offset is free: u and a u give the same transport plan).
+ * params: in = initial values, out = trained (shift/scale set from the
+ * training set).  loss_out: per-epoch mean loss (may be null). */
+wmd_status wmd_ws_train(wmd_handle* h, float* params, int epochs,
+                        uint64_t batch_groups, float lr, uint64_t seed,
+                        double* loss_out);
+/* Loss and gradient of every parameter over given raw feature rows X
+ * [rows][F] (host), targets t [rows], groups gptr [ngroups + 1]: the
+ * training kernels on caller data (for gradient checks). */
+wmd_status wmd_ws_loss_grad(wmd_handle* h, uint64_t d, const float* X,
+                            const float* t, const int64_t* gptr, uint64_t ngroups,
+                            const float* params, double* loss, float* grad);
+/* Read back the training set built last (any pointer may be NULL): the
+ * standardised rows X [rows][F], labels y [rows] (log u), group pointers
+ * [groups + 1], per group the source index and target document, per row the
+ * source word's index within its source. */
+wmd_status wmd_ws_get_training_set(wmd_handle* h, float* X, float* y, int64_t* gptr,
+                                   uint32_t* group_source, uint32_t* group_doc,
+                                   int32_t* row_word);
+/* Use a model for subsequent queries (params = NULL: back to the cold start). */
+wmd_status wmd_set_warm_start(wmd_handle* h, const float* params);
+/* The initial scalings the model gives a dense source r: u0_out [N][v_r]
+ * (host, FP32), v_r written to vr_out. */
+wmd_status wmd_ws_init_scalings(wmd_handle* h, const double* r, double lambda,
+                                float* u0_out, uint64_t* vr_out);
+
 #ifdef __cplusplus
 }
 #endif

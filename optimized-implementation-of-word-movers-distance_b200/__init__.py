@@ -119,6 +119,40 @@ def sinkhorn_wmd(r, c, vecs, lamb, max_iter):
     return np.asmatrix(out.reshape(1, -1))
 
 
+def _pack_sources(sources):
+    """(ptr, ids, weights) of a list of dense histograms or (ids, weights)
+    pairs, ids ascending within each source."""
+    ptr = [0]
+    ids, ws = [], []
+    for src in sources:
+        if isinstance(src, tuple):
+            i, w = np.asarray(src[0], np.uint64), np.asarray(src[1], np.float64)
+            order = np.argsort(i, kind="stable")
+            i, w = i[order], w[order]
+        else:
+            r = np.asarray(src, np.float64)
+            i = np.nonzero(r)[0].astype(np.uint64)
+            w = r[i.astype(np.int64)]
+        ids.append(i)
+        ws.append(w)
+        ptr.append(ptr[-1] + i.size)
+    ptr = np.asarray(ptr, np.uint64)
+    ids = np.ascontiguousarray(np.concatenate(ids) if ids else np.zeros(0), np.uint64)
+    ws = np.ascontiguousarray(np.concatenate(ws) if ws else np.zeros(0), np.float64)
+    return ptr, ids, ws
+
+
+def ws_param_count(d: int) -> int:
+    """Length of the warm-start parameter vector for embedding width d."""
+    return int(lib().wmd_ws_param_count(int(d)))
+
+
+def ws_init_params(d: int, seed: int = 0) -> np.ndarray:
+    p = np.empty(ws_param_count(d), np.float32)
+    check(lib().wmd_ws_init_params(int(d), int(seed), _ptr(p, ctypes.c_float)))
+    return p
+
+
 class Engine:
     """Resident-corpus solver (handle API of include/wmd_b200.h).  ``lam`` is
     the positive regulariser: K = exp(-lam * M)."""
@@ -229,23 +263,7 @@ class Engine:
         """sources: list of dense histograms r (length V) or of (ids,
         weights) pairs.  Returns a (len(sources), N) array of scores (and the
         per-document iteration counts if want_iters)."""
-        ptr = [0]
-        ids, ws = [], []
-        for src in sources:
-            if isinstance(src, tuple):
-                i, w = np.asarray(src[0], np.uint64), np.asarray(src[1], np.float64)
-                order = np.argsort(i, kind="stable")
-                i, w = i[order], w[order]
-            else:
-                r = np.asarray(src, np.float64)
-                i = np.nonzero(r)[0].astype(np.uint64)
-                w = r[i.astype(np.int64)]
-            ids.append(i)
-            ws.append(w)
-            ptr.append(ptr[-1] + i.size)
-        ptr = np.asarray(ptr, np.uint64)
-        ids = np.ascontiguousarray(np.concatenate(ids) if ids else np.zeros(0), np.uint64)
-        ws = np.ascontiguousarray(np.concatenate(ws) if ws else np.zeros(0), np.float64)
+        ptr, ids, ws = _pack_sources(sources)
         S = len(sources)
         out = np.empty((S, self.N), np.float64)
         it = np.empty((S, self.N), np.int32) if want_iters else None
@@ -255,6 +273,85 @@ class Engine:
             _ptr(out, ctypes.c_double),
             it.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if want_iters else None))
         return (out, it) if want_iters else out
+
+    # -- learned warm start -------------------------------------------------
+    def ws_build_training_set(self, sources, lam: float, docs_per_source: int,
+                              words_per_doc: int = 16, label_tol: float = 1e-7,
+                              label_max_iter: int = 5000, seed: int = 0) -> dict:
+        """Converged-FP64 labels for (source, document) pairs of the resident
+        target set; returns {'rows', 'groups', 'mean_label_iters'}."""
+        ptr, ids, ws = _pack_sources(sources)
+        rows, groups = ctypes.c_uint64(), ctypes.c_uint64()
+        mit = ctypes.c_double()
+        check(lib().wmd_ws_build_training_set(
+            self._h, _ptr(ptr, ctypes.c_uint64), _ptr(ids, ctypes.c_uint64),
+            _ptr(ws, ctypes.c_double), len(sources), float(lam), int(docs_per_source),
+            int(words_per_doc), float(label_tol), int(label_max_iter), int(seed),
+            ctypes.byref(rows), ctypes.byref(groups), ctypes.byref(mit)))
+        return {"rows": rows.value, "groups": groups.value,
+                "mean_label_iters": mit.value}
+
+    def ws_train(self, params, epochs: int, batch_groups: int = 256,
+                 lr: float = 1e-3, seed: int = 0):
+        """Adam on the built training set; returns (params, per-epoch loss)."""
+        p = np.ascontiguousarray(params, np.float32).copy()
+        loss = np.empty(int(epochs), np.float64)
+        check(lib().wmd_ws_train(self._h, _ptr(p, ctypes.c_float), int(epochs),
+                                 int(batch_groups), float(lr), int(seed),
+                                 _ptr(loss, ctypes.c_double)))
+        return p, loss
+
+    def ws_loss_grad(self, d: int, X, t, gptr, params):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        gptr = np.ascontiguousarray(gptr, np.int64)
+        params = np.ascontiguousarray(params, np.float32)
+        grad = np.empty_like(params)
+        loss = ctypes.c_double()
+        check(lib().wmd_ws_loss_grad(
+            self._h, int(d), _ptr(X, ctypes.c_float), _ptr(t, ctypes.c_float),
+            gptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), gptr.size - 1,
+            _ptr(params, ctypes.c_float), ctypes.byref(loss), _ptr(grad, ctypes.c_float)))
+        return loss.value, grad
+
+    def ws_training_set(self, info: dict) -> dict:
+        """The built training set (from ws_build_training_set's info):
+        standardised X, labels y, group pointers, per-group source index and
+        document, per-row source-word index."""
+        rows, groups = int(info["rows"]), int(info["groups"])
+        d = int(self.d)
+        F = ((2 * d + 5) + 15) // 16 * 16
+        X = np.empty((rows, F), np.float32)
+        y = np.empty(rows, np.float32)
+        gptr = np.empty(groups + 1, np.int64)
+        gs = np.empty(groups, np.uint32)
+        gd = np.empty(groups, np.uint32)
+        rw = np.empty(rows, np.int32)
+        u32 = ctypes.POINTER(ctypes.c_uint32)
+        check(lib().wmd_ws_get_training_set(
+            self._h, _ptr(X, ctypes.c_float), _ptr(y, ctypes.c_float),
+            gptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            gs.ctypes.data_as(u32), gd.ctypes.data_as(u32),
+            rw.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return {"X": X, "y": y, "gptr": gptr, "source": gs, "doc": gd, "word": rw}
+
+    def set_warm_start(self, params):
+        """Start queries from the model's prediction (None: cold start)."""
+        if params is None:
+            check(lib().wmd_set_warm_start(self._h, None))
+        else:
+            p = np.ascontiguousarray(params, np.float32)
+            check(lib().wmd_set_warm_start(self._h, _ptr(p, ctypes.c_float)))
+
+    def ws_init_scalings(self, r, lam: float) -> np.ndarray:
+        """The model's initial scalings u0 [N][v_r] for a dense source r."""
+        r = _f64(r)
+        vr_max = int(np.count_nonzero(r))
+        u0 = np.empty((self.N, max(vr_max, 1)), np.float32)
+        vr = ctypes.c_uint64()
+        check(lib().wmd_ws_init_scalings(self._h, _ptr(r, ctypes.c_double), float(lam),
+                                         _ptr(u0, ctypes.c_float), ctypes.byref(vr)))
+        return u0[:, :vr.value]
 
     def query_device(self, r_dev_ptr: int, vr_cap: int, lam: float,
                      max_iter: int, out_dev_ptr: int):

@@ -15,6 +15,7 @@ c_u64 = ctypes.c_uint64
 c_f64p = ctypes.POINTER(ctypes.c_double)
 c_f32p = ctypes.POINTER(ctypes.c_float)
 c_u64p = ctypes.POINTER(ctypes.c_uint64)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
 
 STATUS = {
     0: "WMD_OK", 1: "WMD_ERR_INVALID_ARG", 2: "WMD_ERR_INVALID_INPUT",
@@ -68,6 +69,24 @@ _SIGS = [
     ("wmd_set_targets_csr", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSR)]),
     ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_solve_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_ws_param_count", ctypes.c_uint64, [ctypes.c_uint64]),
+    ("wmd_ws_init_params", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, c_f32p]),
+    ("wmd_ws_build_training_set", ctypes.c_int,
+     [ctypes.c_void_p, c_u64p, c_u64p, c_f64p, ctypes.c_uint64, ctypes.c_double,
+      ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_int,
+      ctypes.c_uint64, c_u64p, c_u64p, c_f64p]),
+    ("wmd_ws_train", ctypes.c_int,
+     [ctypes.c_void_p, c_f32p, ctypes.c_int, ctypes.c_uint64, ctypes.c_float,
+      ctypes.c_uint64, c_f64p]),
+    ("wmd_ws_loss_grad", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint64, c_f32p, c_f32p, c_i64p, ctypes.c_uint64, c_f32p,
+      c_f64p, c_f32p]),
+    ("wmd_ws_get_training_set", ctypes.c_int,
+     [ctypes.c_void_p, c_f32p, c_f32p, c_i64p, ctypes.POINTER(ctypes.c_uint32),
+      ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_int32)]),
+    ("wmd_set_warm_start", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
+    ("wmd_ws_init_scalings", ctypes.c_int,
+     [ctypes.c_void_p, c_f64p, ctypes.c_double, c_f32p, c_u64p]),
     ("wmd_query_dense", ctypes.c_int,
      [ctypes.c_void_p, c_f64p, ctypes.c_double, ctypes.c_int, c_f64p]),
     ("wmd_query_dense_device", ctypes.c_int,

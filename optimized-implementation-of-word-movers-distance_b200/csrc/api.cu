@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <random>
 #include <vector>
 
 #include "wmd_b200.h"
@@ -42,6 +43,10 @@ wmd_status fail_cuda(cudaError_t e, const char* what) {
 struct DevBuf {
   void* p = nullptr;
   size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
   cudaError_t ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
     if (p) cudaFree(p);
@@ -86,13 +91,13 @@ struct QueryKey {
   uint64_t epoch = 0;
   float tol = 0.f;
   int prec = -1;
-  const void* bufs[14] = {};  // every device buffer the graph reads or writes
+  const void* bufs[16] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
           epoch == o.epoch && tol == o.tol && prec == o.prec))
       return false;
-    for (int i = 0; i < 14; ++i)
+    for (int i = 0; i < 16; ++i)
       if (bufs[i] != o.bufs[i]) return false;
     return true;
   }
@@ -126,6 +131,20 @@ struct wmd_handle {
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
   // top-k
   DevBuf topk_scratch, topk_idx, topk_val;
+  // learned warm start: model (FP32 parameters, folded inference form),
+  // per-target-set tables, per-query scratch
+  DevBuf ws_params, ws_folded, ws_C, ws_Bdoc, ws_Asrc, ws_u0;
+  bool ws_on = false;       // queries start from the model's prediction
+  bool ws_docs_ready = false;  // ws_C / ws_Bdoc match targets + model
+  int ws_d = 0;
+  // warm-start training set (standardised rows, labels, group pointers)
+  DevBuf ws_X, ws_y, ws_gptr;
+  std::vector<int64_t> ws_gptr_host;
+  std::vector<uint32_t> ws_gsrc, ws_gdoc;  // per group: source index, document
+  std::vector<int32_t> ws_rword;           // per row: source word index
+  std::vector<float> ws_shift, ws_scale;
+  int64_t ws_rows = 0;
+  std::vector<uint32_t> doc_len;  // host copy of the target lengths
   float tol = 0.f;  // per-document convergence tolerance (0: fixed count)
   unsigned* err_host = nullptr;      // pinned
   uint32_t* chunks_host = nullptr;   // pinned, grown with V
@@ -204,6 +223,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
   h->d = d;
   h->have_E = true;
   h->e16_fmt = -1;
+  h->ws_docs_ready = false;
   h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
@@ -274,6 +294,9 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   h->N = N;
   h->nnz = nnz;
   h->have_T = true;
+  h->ws_docs_ready = false;
+  h->doc_len.resize(N);
+  for (uint64_t j = 0; j < N; ++j) h->doc_len[j] = (uint32_t)(c->col_ptr[j + 1] - c->col_ptr[j]);
   h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
@@ -310,6 +333,22 @@ wmd_status csr_to_csc_host(const wmd_csr_double_t* a, std::vector<uint64_t>& cp,
       rows[pos] = w;
       vals[pos] = a->vals[e];
     }
+  return WMD_OK;
+}
+
+// Warm start: target centroids and the per-document first-layer terms of the
+// current model (recomputed after the targets, embeddings or model change).
+wmd_status ws_prepare_docs(wmd_handle* h) {
+  if (h->ws_docs_ready) return WMD_OK;
+  const WsLayout L = ws_layout((int)h->d);
+  CK(h->ws_C.ensure((size_t)h->N * h->d * sizeof(float)));
+  CK(h->ws_Bdoc.ensure((size_t)h->N * kWsH * sizeof(float)));
+  launch_centroids(h->E32.as<float>(), (int)h->d, h->col_ptr.as<int64_t>(),
+                   h->ent.as<uint2>(), (int64_t)h->N, h->ws_C.as<float>(), h->stream);
+  launch_ws_doc_bias(L, h->ws_folded.as<float>(), h->ws_C.as<float>(), (int64_t)h->N,
+                     h->ws_Bdoc.as<float>(), h->stream);
+  CK(cudaGetLastError());
+  h->ws_docs_ready = true;
   return WMD_OK;
 }
 
@@ -376,6 +415,14 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   near.E32 = h->E32.as<float>();
   near.S32 = sel.S;
   near.d = (int)d;
+  // Learned warm start (needs lambda != 0: its features read M = ln K / expo).
+  const bool ws = h->ws_on && h->ws_d == (int)d && expo != 0.f;
+  if (ws) {
+    wmd_status sw = ws_prepare_docs(h);
+    if (sw) return sw;
+    CK(h->ws_Asrc.ensure((size_t)std::max<uint32_t>(cap, 1) * kWsH * sizeof(float)));
+    CK(h->ws_u0.ensure((size_t)std::max<uint64_t>(h->N, 1) * ld * sizeof(float)));
+  }
   // Everything below is stream work only (no allocation, no host sync), so
   // it can be captured into a CUDA graph and replayed.
   auto record = [&](int i, bool capturing) -> cudaError_t {
@@ -407,16 +454,25 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     }
     n += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
                            h->nE.as<float>(), sel.nS, sel.vr, h->sms, h->stream);
-    CK(record(2, capturing));
     SolveCtl ctl;
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->iters.as<int>();
+    if (ws) {
+      n += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
+                          h->ws_params.as<float>(), sel.S, sel.rinv, (int)cap,
+                          h->K.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
+                          h->ws_Asrc.as<float>(), h->ws_u0.as<float>(), ld,
+                          h->err_dev.as<unsigned>(), h->sms, h->stream);
+      ctl.u0 = h->ws_u0.as<float>();
+      ctl.ldu = ld;
+    }
+    CK(record(2, capturing));
     if (ld16) {
       n += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V, sel.vr,
                                 h->sms, h->stream);
       const int ls = launch_solve_block(h->K16.p, ld16, expo, cap, sel, t, ctl,
-                                        nullptr, 0, out_dev, h->stream);
+                                        ctl.u0, ctl.ldu, out_dev, h->stream);
       if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "block solve unavailable");
       n += ls;
     } else {
@@ -442,12 +498,13 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.timing = h->timing;
   key.epoch = h->graph_epoch;
   key.tol = h->tol;
-  key.prec = (int)h->prec;
+  key.prec = (int)h->prec + (ws ? 2 : 0);
   {
-    const DevBuf* used[14] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+    const DevBuf* used[16] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
                               &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
-                              &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16};
-    for (int i = 0; i < 14; ++i) key.bufs[i] = used[i]->p;
+                              &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16,
+                              &h->ws_Asrc, &h->ws_u0};
+    for (int i = 0; i < 16; ++i) key.bufs[i] = used[i]->p;
   }
   if (!h->use_graphs) {
     int n = 0;
@@ -611,6 +668,13 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   if (h->prec == WMD_SOLVE_BF16 && !need_km)
     for (uint64_t s = 0; s < S; ++s) ld16_max = std::max(ld16_max, block_panel_width(vrs[s]));
   if (ld16_max) CK(h->K16.ensure((size_t)V * ld16_max * 2));
+  const bool ws = h->ws_on && h->ws_d == (int)d && expo != 0.f;
+  if (ws) {
+    wmd_status sw = ws_prepare_docs(h);
+    if (sw) return sw;
+    CK(h->ws_Asrc.ensure((size_t)vr_max * kWsH * sizeof(float)));
+    CK(h->ws_u0.ensure((size_t)std::max<uint64_t>(N, 1) * ld_max * sizeof(float)));
+  }
   const unsigned near_cap = (unsigned)std::min<uint64_t>((uint64_t)V * vr_max, 1u << 20);
   CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
   CK(h->near_count.ensure(sizeof(unsigned)));
@@ -683,12 +747,21 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->b_iters.as<int>() + s * N;
+    if (ws && vr > 0) {
+      launches += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
+                                 h->ws_params.as<float>(), sel.S, sel.rinv, (int)vr,
+                                 h->K.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
+                                 h->ws_Asrc.as<float>(), h->ws_u0.as<float>(), ld,
+                                 h->err_dev.as<unsigned>(), h->sms, h->stream);
+      ctl.u0 = h->ws_u0.as<float>();
+      ctl.ldu = ld;
+    }
     const int ld16 = h->prec == WMD_SOLVE_BF16 && !KMp ? block_panel_width(vr) : 0;
     int ls;
     if (ld16) {
       launches += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V,
                                        sel.vr, h->sms, h->stream);
-      ls = launch_solve_block(h->K16.p, ld16, expo, vr, sel, t, ctl, nullptr, 0,
+      ls = launch_solve_block(h->K16.p, ld16, expo, vr, sel, t, ctl, ctl.u0, ctl.ldu,
                               h->b_out.as<double>() + s * N, h->stream);
     } else {
       ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
@@ -839,7 +912,9 @@ wmd_status wmd_destroy(wmd_handle* h) {
                     &h->sel_chunks, &h->K, &h->KM, &h->out_dev, &h->err_dev,
                     &h->near_pairs, &h->near_count, &h->iters, &h->b_ids,
                     &h->b_rinv, &h->b_vr, &h->b_out, &h->b_iters,
-                    &h->topk_scratch, &h->topk_idx, &h->topk_val})
+                    &h->topk_scratch, &h->topk_idx, &h->topk_val, &h->K16,
+                    &h->ws_params, &h->ws_folded, &h->ws_C, &h->ws_Bdoc,
+                    &h->ws_Asrc, &h->ws_u0, &h->ws_X, &h->ws_y, &h->ws_gptr})
     b->release();
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->chunks_host) cudaFreeHost(h->chunks_host);
@@ -1051,6 +1126,413 @@ wmd_status wmd_sinkhorn_nonfused_csc(const double* r, const double* vecs,
                                      const wmd_csc_double_t* c_csc) {
   return dropin_csc(r, vecs, WMD, (float)(-lamda), max_iter, data_vocab_size,
                     num_docs, word2vec_word_embedding_size, c_csc);
+}
+
+/* ------------------------------------------------------------------------
+ * Learned warm start.
+ * ---------------------------------------------------------------------- */
+
+uint64_t wmd_ws_param_count(uint64_t d) {
+  if (d == 0 || d > 65536) return 0;
+  return (uint64_t)ws_layout((int)d).count;
+}
+
+wmd_status wmd_ws_init_params(uint64_t d, uint64_t seed, float* params) {
+  if (!params || d == 0 || d > 65536) return fail(WMD_ERR_INVALID_ARG, "bad argument");
+  const WsLayout L = ws_layout((int)d);
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  std::fill(params, params + L.count, 0.f);
+  for (int f = 0; f < L.F; ++f) params[L.scale + f] = 1.f;
+  const float s1 = 1.f / std::sqrt((float)L.F), s2 = 1.f / std::sqrt((float)kWsH);
+  for (size_t i = 0; i < (size_t)kWsH * L.F; ++i) params[L.W1 + i] = s1 * nd(rng);
+  for (size_t i = 0; i < (size_t)kWsH * kWsH; ++i) params[L.W2 + i] = s2 * nd(rng);
+  for (int i = 0; i < kWsH; ++i) params[L.w3 + i] = s2 * nd(rng);
+  return WMD_OK;
+}
+
+wmd_status wmd_ws_build_training_set(wmd_handle* h, const uint64_t* src_ptr,
+                                     const uint64_t* src_ids, const double* src_w,
+                                     uint64_t S, double lambda,
+                                     uint32_t docs_per_source, uint32_t words_per_doc,
+                                     double label_tol, int label_max_iter,
+                                     uint64_t seed, uint64_t* rows_out,
+                                     uint64_t* groups_out, double* mean_label_iters) {
+  if (!h || !src_ptr || S == 0 || docs_per_source == 0 || words_per_doc == 0 ||
+      label_max_iter <= 0 || !(label_tol > 0.0) || lambda == 0.0)
+    return fail(WMD_ERR_INVALID_ARG, "bad argument");
+  if (!h->have_E || !h->have_T || h->tV != h->V)
+    return fail(WMD_ERR_INVALID_ARG, "embeddings and targets must be set first");
+  wmd_status st = bind(h);
+  if (st) return st;
+  const uint64_t V = h->V, d = h->d, N = h->N;
+  const WsLayout L = ws_layout((int)d);
+  const float expo = (float)(-lambda);
+  std::vector<int32_t> nonempty;
+  for (uint64_t j = 0; j < N; ++j)
+    if (h->doc_len[j] > 0) nonempty.push_back((int32_t)j);
+  if (nonempty.empty()) return fail(WMD_ERR_INVALID_INPUT, "no non-empty target document");
+  const uint32_t D = std::min<uint64_t>(docs_per_source, nonempty.size());
+  const int G = (int)words_per_doc;
+  // Upper bound of the rows, then the buffers.
+  uint64_t maxrows = 0, vr_max = 1;
+  for (uint64_t s = 0; s < S; ++s) {
+    if (src_ptr[s + 1] < src_ptr[s]) return fail(WMD_ERR_INVALID_INPUT, "source pointers decrease");
+    const uint64_t vr = src_ptr[s + 1] - src_ptr[s];
+    if (vr > 512) return fail(WMD_ERR_UNSUPPORTED, "training sources must have <= 512 words");
+    for (uint64_t e = src_ptr[s]; e < src_ptr[s + 1]; ++e) {
+      if (src_ids[e] >= V) return fail(WMD_ERR_INVALID_INPUT, "source word id >= V");
+      if (e > src_ptr[s] && src_ids[e] <= src_ids[e - 1])
+        return fail(WMD_ERR_INVALID_INPUT, "source word ids not strictly ascending");
+      if (!(src_w[e] > 0.0) || !std::isfinite(src_w[e]))
+        return fail(WMD_ERR_INVALID_INPUT, "source weight <= 0 or not finite");
+    }
+    maxrows += (uint64_t)D * std::min<uint64_t>(vr, (uint64_t)G);
+    vr_max = std::max(vr_max, vr);
+  }
+  const int ld_max = (int)((vr_max + 3) & ~3ull);
+  CK(h->ws_C.ensure((size_t)N * d * sizeof(float)));
+  CK(h->ws_X.ensure((size_t)std::max<uint64_t>(maxrows, 1) * L.F * sizeof(float)));
+  CK(h->ws_y.ensure((size_t)std::max<uint64_t>(maxrows, 1) * sizeof(float)));
+  CK(h->K.ensure((size_t)V * ld_max * sizeof(float)));
+  CK(h->sel_S.ensure((size_t)vr_max * d * sizeof(float)));
+  CK(h->sel_nS.ensure((size_t)vr_max * sizeof(float)));
+  const unsigned near_cap = (unsigned)std::min<uint64_t>((uint64_t)V * vr_max, 1u << 20);
+  CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
+  CK(h->near_count.ensure(sizeof(unsigned)));
+  DevBuf ids_d, r64_d, rinv_d, docs_d, u_d, it_d, res_d, sel_d, row0_d, vrd;
+  CK(ids_d.ensure(vr_max * 4));
+  CK(r64_d.ensure(vr_max * 8));
+  CK(rinv_d.ensure(vr_max * 4));
+  CK(vrd.ensure(4));
+  CK(docs_d.ensure((size_t)D * 4));
+  CK(u_d.ensure((size_t)D * vr_max * 8));
+  CK(it_d.ensure((size_t)D * 4));
+  CK(res_d.ensure((size_t)D * 8));
+  CK(sel_d.ensure((size_t)D * G * 4));
+  CK(row0_d.ensure((size_t)D * 8));
+  launch_centroids(h->E32.as<float>(), (int)d, h->col_ptr.as<int64_t>(),
+                   h->ent.as<uint2>(), (int64_t)N, h->ws_C.as<float>(), h->stream);
+  Targets t;
+  t.col_ptr = h->col_ptr.as<int64_t>();
+  t.ent = h->ent.as<uint2>();
+  t.N = (int64_t)N;
+  t.nnz = (int64_t)h->nnz;
+  std::mt19937_64 rng(seed);
+  std::vector<int64_t> gptr(1, 0);
+  std::vector<uint32_t> gsrc, gdoc;
+  std::vector<int32_t> rword;
+  int64_t rows = 0;
+  double it_sum = 0.0;
+  uint64_t it_cnt = 0;
+  std::vector<int32_t> docs(D), sel((size_t)D * G);
+  std::vector<int> its(D);
+  std::vector<double> res(D);
+  std::vector<int64_t> row0(D);
+  std::vector<uint32_t> ids32;
+  std::vector<float> rinv;
+  for (uint64_t s = 0; s < S; ++s) {
+    const uint64_t off = src_ptr[s];
+    const uint32_t vr = (uint32_t)(src_ptr[s + 1] - off);
+    if (vr == 0) continue;
+    const int ld = (int)((vr + 3) & ~3u);
+    ids32.assign(vr, 0);
+    rinv.assign(vr, 0.f);
+    for (uint32_t i = 0; i < vr; ++i) {
+      ids32[i] = (uint32_t)src_ids[off + i];
+      rinv[i] = (float)(1.0 / src_w[off + i]);
+    }
+    CK(cudaMemcpyAsync(ids_d.p, ids32.data(), vr * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(r64_d.p, src_w + off, vr * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(rinv_d.p, rinv.data(), vr * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(vrd.p, &vr, 4, cudaMemcpyHostToDevice, h->stream));
+    SourceSel sel_s;
+    sel_s.ids = ids_d.as<uint32_t>();
+    sel_s.rinv = rinv_d.as<float>();
+    sel_s.S = h->sel_S.as<float>();
+    sel_s.nS = h->sel_nS.as<float>();
+    sel_s.vr = vrd.as<uint32_t>();
+    sel_s.cap = vr;
+    NearList near;
+    near.pairs = h->near_pairs.as<uint2>();
+    near.count = h->near_count.as<unsigned>();
+    near.cap = near_cap;
+    near.E32 = h->E32.as<float>();
+    near.S32 = sel_s.S;
+    near.d = (int)d;
+    launch_gather_sources(sel_s.ids, (int)vr, h->E32.as<float>(), h->nE.as<float>(), d,
+                          sel_s.S, sel_s.nS, nullptr, nullptr, 0, h->stream);
+    CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
+    launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d, sel_s, expo,
+                      h->K.as<float>(), nullptr, ld, near, h->stream);
+    launch_near_fixup(near, expo, h->K.as<float>(), nullptr, ld, V, h->nE.as<float>(),
+                      sel_s.nS, sel_s.vr, h->sms, h->stream);
+    // documents of this source: a seeded sample without replacement
+    for (uint32_t q = 0; q < D; ++q) {
+      const uint64_t k = q + rng() % (nonempty.size() - q);
+      std::swap(nonempty[q], nonempty[k]);
+      docs[q] = nonempty[q];
+    }
+    CK(cudaMemcpyAsync(docs_d.p, docs.data(), D * 4, cudaMemcpyHostToDevice, h->stream));
+    if (launch_solve_f64(h->K.as<float>(), ld, (int)vr, r64_d.as<double>(),
+                         t.col_ptr, t.ent, docs_d.as<int32_t>(), (int)D, label_tol,
+                         label_max_iter, u_d.as<double>(), it_d.as<int>(),
+                         res_d.as<double>(), h->stream) < 0)
+      return fail(WMD_ERR_UNSUPPORTED, "label solve: too many source words");
+    CK(cudaMemcpyAsync(its.data(), it_d.p, D * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(res.data(), res_d.p, D * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int g = std::min<int>(G, (int)vr);
+    const uint32_t stride = vr / (uint32_t)g;
+    for (uint32_t q = 0; q < D; ++q) {
+      const bool keep = res[q] <= label_tol;
+      row0[q] = keep ? rows : -1;
+      const uint32_t rot = (uint32_t)(rng() % vr);
+      for (int m = 0; m < G; ++m)
+        sel[(size_t)q * G + m] = (keep && m < g) ? (int32_t)((rot + m * stride) % vr) : -1;
+      if (keep) {
+        rows += g;
+        gptr.push_back(rows);
+        gsrc.push_back((uint32_t)s);
+        gdoc.push_back((uint32_t)docs[q]);
+        for (int m = 0; m < g; ++m) rword.push_back(sel[(size_t)q * G + m]);
+        it_sum += its[q];
+        ++it_cnt;
+      }
+    }
+    CK(cudaMemcpyAsync(sel_d.p, sel.data(), (size_t)D * G * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(row0_d.p, row0.data(), (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
+    launch_ws_rows(h->E32.as<float>(), (int)d, h->ws_C.as<float>(), h->K.as<float>(), ld,
+                   expo, ids_d.as<uint32_t>(), r64_d.as<double>(), (int)vr, t.col_ptr,
+                   t.ent, docs_d.as<int32_t>(), u_d.as<double>(), (int)D,
+                   sel_d.as<int32_t>(), G, row0_d.as<int64_t>(), L.F,
+                   h->ws_X.as<float>(), h->ws_y.as<float>(), h->stream);
+    CK(cudaStreamSynchronize(h->stream));  // host vectors reused next source
+    CK(cudaGetLastError());
+  }
+  if (rows == 0) return fail(WMD_ERR_INVALID_INPUT, "no labelled document converged");
+  // Standardisation statistics (FP64 partial sums), then X in place.
+  const int chunks = 256;
+  DevBuf s1, s2;
+  CK(s1.ensure((size_t)chunks * L.F * 8));
+  CK(s2.ensure((size_t)chunks * L.F * 8));
+  launch_ws_colstats(h->ws_X.as<float>(), rows, L.F, s1.as<double>(), s2.as<double>(),
+                     chunks, h->stream);
+  std::vector<double> a((size_t)chunks * L.F), b((size_t)chunks * L.F);
+  CK(cudaMemcpyAsync(a.data(), s1.p, a.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(b.data(), s2.p, b.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->ws_shift.assign(L.F, 0.f);
+  h->ws_scale.assign(L.F, 1.f);
+  for (int f = 0; f < L.F; ++f) {
+    double m = 0.0, q = 0.0;
+    for (int c = 0; c < chunks; ++c) {
+      m += a[(size_t)c * L.F + f];
+      q += b[(size_t)c * L.F + f];
+    }
+    m /= (double)rows;
+    const double var = std::max(q / (double)rows - m * m, 0.0);
+    h->ws_shift[f] = (float)m;
+    h->ws_scale[f] = var > 1e-12 ? (float)(1.0 / std::sqrt(var)) : 1.f;
+  }
+  DevBuf sh, sc;
+  CK(sh.ensure(L.F * 4));
+  CK(sc.ensure(L.F * 4));
+  CK(cudaMemcpyAsync(sh.p, h->ws_shift.data(), L.F * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(sc.p, h->ws_scale.data(), L.F * 4, cudaMemcpyHostToDevice, h->stream));
+  launch_ws_standardize(h->ws_X.as<float>(), rows, L.F, sh.as<float>(), sc.as<float>(),
+                        h->stream);
+  h->ws_gptr_host = gptr;
+  h->ws_gsrc = gsrc;
+  h->ws_gdoc = gdoc;
+  h->ws_rword = rword;
+  CK(h->ws_gptr.ensure(gptr.size() * 8));
+  CK(cudaMemcpyAsync(h->ws_gptr.p, gptr.data(), gptr.size() * 8, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  h->ws_rows = rows;
+  h->ws_d = (int)d;
+  if (rows_out) *rows_out = (uint64_t)rows;
+  if (groups_out) *groups_out = gptr.size() - 1;
+  if (mean_label_iters) *mean_label_iters = it_cnt ? it_sum / (double)it_cnt : 0.0;
+  return WMD_OK;
+}
+
+wmd_status wmd_ws_train(wmd_handle* h, float* params, int epochs,
+                        uint64_t batch_groups, float lr, uint64_t seed,
+                        double* loss_out) {
+  if (!h || !params || epochs <= 0 || batch_groups == 0 || !(lr > 0.f))
+    return fail(WMD_ERR_INVALID_ARG, "bad argument");
+  if (h->ws_rows == 0) return fail(WMD_ERR_INVALID_ARG, "no training set built");
+  wmd_status st = bind(h);
+  if (st) return st;
+  const WsLayout L = ws_layout(h->ws_d);
+  // The model's standardisation is the training set's.
+  std::copy(h->ws_shift.begin(), h->ws_shift.end(), params + L.shift);
+  std::copy(h->ws_scale.begin(), h->ws_scale.end(), params + L.scale);
+  const int64_t ngroups = (int64_t)h->ws_gptr_host.size() - 1;
+  int64_t maxg = 0;
+  for (int64_t g = 0; g < ngroups; ++g)
+    maxg = std::max(maxg, h->ws_gptr_host[g + 1] - h->ws_gptr_host[g]);
+  const int64_t bmax = (int64_t)std::min<uint64_t>(batch_groups, ngroups) * maxg;
+  DevBuf P, Gd, M1, M2, Xb, tb, bp, perm_d, scr, lossg;
+  CK(P.ensure(L.count * 4));
+  CK(Gd.ensure(L.count * 4));
+  CK(M1.ensure(L.count * 4));
+  CK(M2.ensure(L.count * 4));
+  CK(Xb.ensure((size_t)bmax * L.F * 4));
+  CK(tb.ensure((size_t)bmax * 4));
+  CK(bp.ensure((size_t)(batch_groups + 1) * 8));
+  CK(perm_d.ensure((size_t)ngroups * 8));
+  CK(scr.ensure(ws_scratch_floats(bmax, L.F) * 4));
+  CK(lossg.ensure((size_t)batch_groups * 8));
+  CK(cudaMemcpyAsync(P.p, params, L.count * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(M1.p, 0, L.count * 4, h->stream));
+  CK(cudaMemsetAsync(M2.p, 0, L.count * 4, h->stream));
+  std::vector<int64_t> perm(ngroups), bptr;
+  std::vector<double> lg(batch_groups);
+  std::mt19937_64 rng(seed);
+  int step = 0;
+  for (int ep = 0; ep < epochs; ++ep) {
+    for (int64_t g = 0; g < ngroups; ++g) perm[g] = g;
+    std::shuffle(perm.begin(), perm.end(), rng);
+    CK(cudaMemcpyAsync(perm_d.p, perm.data(), ngroups * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double loss = 0.0;
+    for (int64_t g0 = 0; g0 < ngroups; g0 += (int64_t)batch_groups) {
+      const int64_t ng = std::min<int64_t>((int64_t)batch_groups, ngroups - g0);
+      bptr.assign(ng + 1, 0);
+      for (int64_t q = 0; q < ng; ++q) {
+        const int64_t g = perm[g0 + q];
+        bptr[q + 1] = bptr[q] + (h->ws_gptr_host[g + 1] - h->ws_gptr_host[g]);
+      }
+      const int64_t rows = bptr[ng];
+      CK(cudaMemcpyAsync(bp.p, bptr.data(), (ng + 1) * 8, cudaMemcpyHostToDevice, h->stream));
+      launch_ws_gather(h->ws_X.as<float>(), h->ws_y.as<float>(), h->ws_gptr.as<int64_t>(),
+                       perm_d.as<int64_t>(), bp.as<int64_t>(), g0, ng, L.F,
+                       Xb.as<float>(), tb.as<float>(), h->stream);
+      launch_ws_fwd_bwd(L, P.as<float>(), Xb.as<float>(), tb.as<float>(), bp.as<int64_t>(),
+                        ng, rows, Gd.as<float>(), lossg.as<double>(), scr.as<float>(),
+                        h->stream);
+      launch_ws_adam(L, P.as<float>(), Gd.as<float>(), M1.as<float>(), M2.as<float>(), lr,
+                     ++step, h->stream);
+      CK(cudaMemcpyAsync(lg.data(), lossg.p, ng * 8, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));  // bptr / lg reused next batch
+      CK(cudaGetLastError());
+      double bl = 0.0;
+      for (int64_t q = 0; q < ng; ++q) bl += lg[q];
+      loss += bl * (double)rows;
+    }
+    if (loss_out) loss_out[ep] = loss / (double)h->ws_rows;
+  }
+  CK(cudaMemcpyAsync(params, P.p, L.count * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return WMD_OK;
+}
+
+wmd_status wmd_ws_loss_grad(wmd_handle* h, uint64_t d, const float* X,
+                            const float* t, const int64_t* gptr, uint64_t ngroups,
+                            const float* params, double* loss, float* grad) {
+  if (!h || !X || !t || !gptr || ngroups == 0 || !params || !loss || !grad || d == 0)
+    return fail(WMD_ERR_INVALID_ARG, "bad argument");
+  wmd_status st = bind(h);
+  if (st) return st;
+  const WsLayout L = ws_layout((int)d);
+  const int64_t rows = gptr[ngroups];
+  if (rows <= 0 || gptr[0] != 0) return fail(WMD_ERR_INVALID_ARG, "bad group pointers");
+  DevBuf P, Gd, Xd, td, gp, scr, lossg;
+  CK(P.ensure(L.count * 4));
+  CK(Gd.ensure(L.count * 4));
+  CK(Xd.ensure((size_t)rows * L.F * 4));
+  CK(td.ensure((size_t)rows * 4));
+  CK(gp.ensure((ngroups + 1) * 8));
+  CK(scr.ensure(ws_scratch_floats(rows, L.F) * 4));
+  CK(lossg.ensure(ngroups * 8));
+  CK(cudaMemcpyAsync(P.p, params, L.count * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(Xd.p, X, (size_t)rows * L.F * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(td.p, t, (size_t)rows * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(gp.p, gptr, (ngroups + 1) * 8, cudaMemcpyHostToDevice, h->stream));
+  launch_ws_standardize(Xd.as<float>(), rows, L.F, P.as<float>() + L.shift,
+                        P.as<float>() + L.scale, h->stream);
+  launch_ws_fwd_bwd(L, P.as<float>(), Xd.as<float>(), td.as<float>(), gp.as<int64_t>(),
+                    (int64_t)ngroups, rows, Gd.as<float>(), lossg.as<double>(),
+                    scr.as<float>(), h->stream);
+  std::vector<double> lg(ngroups);
+  CK(cudaMemcpyAsync(grad, Gd.p, L.count * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(lg.data(), lossg.p, ngroups * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  double l = 0.0;
+  for (uint64_t g = 0; g < ngroups; ++g) l += lg[g];
+  *loss = l;
+  return WMD_OK;
+}
+
+wmd_status wmd_ws_get_training_set(wmd_handle* h, float* X, float* y, int64_t* gptr,
+                                   uint32_t* group_source, uint32_t* group_doc,
+                                   int32_t* row_word) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (h->ws_rows == 0) return fail(WMD_ERR_INVALID_ARG, "no training set built");
+  wmd_status st = bind(h);
+  if (st) return st;
+  const WsLayout L = ws_layout(h->ws_d);
+  if (X) CK(cudaMemcpy(X, h->ws_X.p, (size_t)h->ws_rows * L.F * 4, cudaMemcpyDeviceToHost));
+  if (y) CK(cudaMemcpy(y, h->ws_y.p, (size_t)h->ws_rows * 4, cudaMemcpyDeviceToHost));
+  if (gptr) std::copy(h->ws_gptr_host.begin(), h->ws_gptr_host.end(), gptr);
+  if (group_source) std::copy(h->ws_gsrc.begin(), h->ws_gsrc.end(), group_source);
+  if (group_doc) std::copy(h->ws_gdoc.begin(), h->ws_gdoc.end(), group_doc);
+  if (row_word) std::copy(h->ws_rword.begin(), h->ws_rword.end(), row_word);
+  return WMD_OK;
+}
+
+wmd_status wmd_set_warm_start(wmd_handle* h, const float* params) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  wmd_status st = bind(h);
+  if (st) return st;
+  h->graph_epoch++;
+  h->ws_docs_ready = false;
+  if (!params) {
+    h->ws_on = false;
+    return WMD_OK;
+  }
+  if (!h->have_E) return fail(WMD_ERR_INVALID_ARG, "embeddings must be set first");
+  const WsLayout L = ws_layout((int)h->d);
+  CK(h->ws_params.ensure(L.count * 4));
+  CK(h->ws_folded.ensure(ws_folded_floats(L) * 4));
+  CK(cudaMemcpyAsync(h->ws_params.p, params, L.count * 4, cudaMemcpyHostToDevice,
+                     h->stream));
+  launch_ws_fold(L, h->ws_params.as<float>(), h->ws_folded.as<float>(), h->stream);
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  h->ws_d = (int)h->d;
+  h->ws_on = true;
+  return WMD_OK;
+}
+
+wmd_status wmd_ws_init_scalings(wmd_handle* h, const double* r, double lambda,
+                                float* u0_out, uint64_t* vr_out) {
+  if (!h || !r || !u0_out || !vr_out || lambda == 0.0)
+    return fail(WMD_ERR_INVALID_ARG, "bad argument");
+  if (!h->ws_on) return fail(WMD_ERR_INVALID_ARG, "no warm-start model set");
+  wmd_status st = bind(h);
+  if (st) return st;
+  // A zero-iteration query runs selection, the cost panel and the
+  // warm-start init; the scalings are then read back.
+  const bool g = h->use_graphs;
+  h->use_graphs = false;
+  std::vector<double> scratch(h->N);
+  st = query_host(h, r, (float)(-lambda), 0, scratch.data());
+  h->use_graphs = g;
+  if (st) return st;
+  uint32_t vr = 0;
+  CK(cudaMemcpy(&vr, h->sel_vr.p, 4, cudaMemcpyDeviceToHost));
+  const int ld = (int)(((vr ? vr : 1) + 3u) & ~3u);
+  *vr_out = vr;
+  if (vr == 0) return WMD_OK;
+  CK(cudaMemcpy2D(u0_out, vr * sizeof(float), h->ws_u0.p, ld * sizeof(float),
+                  vr * sizeof(float), h->N, cudaMemcpyDeviceToHost));
+  return WMD_OK;
 }
 
 }  // extern "C"

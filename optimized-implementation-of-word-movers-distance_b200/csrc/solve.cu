@@ -118,6 +118,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              const uint2* __restrict__ ent,
              const int32_t* __restrict__ order, int64_t N, int max_iter,
              float tol, int* __restrict__ iters_out, int srounds,
+             const float* __restrict__ u0, int64_t ldu,
              double* __restrict__ out) {
   using Sh = SolveShape<LPW>;
   constexpr int WPS = Sh::WPS;
@@ -352,30 +353,54 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       for (int qq = 0; qq < LPW; ++qq) uval[qq] = ((dmask >> qq) & 1u) ? (float)vr : 0.f;
       broadcast_u(uval, u2);
     }
-
-    int it = 0;
-    while (it < max_iter) {
+    // One x-update from the u in u2 / ubuf: the new u into unew, and the
+    // marginal residual |u_i (K v)_i - r_i| of the u entering it (read from
+    // the broadcast buffer: each lane reads only entries it wrote itself),
+    // warp-reduced when want_res.
+    auto step = [&](float (&unew)[LPW], bool want_res) {
       float2 x2[16];
       pass(u2, x2);
-      float tot[LPW], uval[LPW];
+      float tot[LPW];
       reduce_slots(x2, tot);
-      // Marginal residual |u_i (K v)_i - r_i| with the u entering this
-      // update (still in the broadcast buffer: each lane reads only the
-      // entries it wrote itself).
       float res = 0.f;
 #pragma unroll
       for (int qq = 0; qq < LPW; ++qq) {
         const bool ok = (dmask >> qq) & 1u;
-        if (tol > 0.f && ok) res += fabsf(ubuf[32 * qq + lane] * tot[qq] - rw[qq]);
-        uval[qq] = ok ? __frcp_rn(rv[qq] * tot[qq]) : 0.f;
+        if (want_res && ok) res += fabsf(ubuf[32 * qq + lane] * tot[qq] - rw[qq]);
+        unew[qq] = ok ? __frcp_rn(rv[qq] * tot[qq]) : 0.f;
       }
-      broadcast_u(uval, u2);
-      ++it;
-      if (tol > 0.f) {
+      if (want_res) {
 #pragma unroll
         for (int off = 16; off; off >>= 1) res += __shfl_xor_sync(0xffffffffu, res, off);
-        if (res <= tol) break;
       }
+      return res;
+    };
+
+    int it = 0;
+    float res = 0.f;
+    if (u0 && max_iter > 0) {
+      // Warm start: the first update from both the cold start and u0; keep
+      // u0's unless its residual is worse than the cold start's or not
+      // finite.
+      float uc[LPW], uw[LPW], uval[LPW];
+      const float rc = step(uc, true);
+#pragma unroll
+      for (int qq = 0; qq < LPW; ++qq)
+        uval[qq] = ((dmask >> qq) & 1u) ? __ldg(&u0[j * ldu + 32 * qq + lane]) : 0.f;
+      broadcast_u(uval, u2);
+      const float rwm = step(uw, true);
+      const bool use_warm = isfinite(rwm) && !(rc < rwm);
+#pragma unroll
+      for (int qq = 0; qq < LPW; ++qq) uval[qq] = use_warm ? uw[qq] : uc[qq];
+      broadcast_u(uval, u2);
+      res = use_warm ? rwm : rc;
+      it = 1;
+    }
+    while (it < max_iter && !(it > 0 && tol > 0.f && res <= tol)) {
+      float uval[LPW];
+      res = step(uval, tol > 0.f);
+      broadcast_u(uval, u2);
+      ++it;
     }
     if (iters_out && lane == 0) iters_out[j] = it;
 
@@ -485,7 +510,7 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   if (grid < 1) grid = 1;
   solve_kernel<LPW, FROM_KM><<<(unsigned)grid, kWarps * 32, smem, st>>>(
       K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
-      ctl.max_iter, ctl.tol, ctl.iters, sr, out);
+      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, out);
   return 1;
 }
 

@@ -162,10 +162,15 @@ int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
 // after the first update whose marginal residual sum_i |u_i (K v)_i - r_i|
 // (measured with the scalings entering that update) is <= tol, or after
 // max_iter updates.  iters (optional, [N]) receives each document's count.
+// u0 (optional, [N][ldu]): initial scaling per document (warm start); the
+// first update is then evaluated from both u0 and the cold start and the one
+// with the smaller marginal residual is kept.
 struct SolveCtl {
   int max_iter = 15;
   float tol = 0.f;
   int* iters = nullptr;
+  const float* u0 = nullptr;
+  int64_t ldu = 0;
 };
 
 // Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
@@ -184,5 +189,52 @@ int launch_panel_to_bf16(const float* K, int ld, void* K16, int ld16, uint64_t V
 int launch_solve_block(const void* K16, int ld16, float expo, uint32_t vr_cap,
                        const SourceSel& s, const Targets& t, const SolveCtl& ctl,
                        const float* u0, int64_t ldu, double* out, cudaStream_t st);
+
+// Learned warm start (warmstart.cu: training, ws_infer.cu: inference).
+// Parameter vector layout (FP32), for embedding width d:
+//   shift [F], scale [F], W1 [256][F], b1 [256], W2 [256][256], b2 [256],
+//   w3 [256], b3 [1] (+3 pad);  F = 2d + 5 rounded up to 16.
+constexpr int kWsH = 256;
+struct WsLayout {
+  int d = 0, F = 0;
+  size_t shift = 0, scale = 0, W1 = 0, b1 = 0, W2 = 0, b2 = 0, w3 = 0, b3 = 0,
+         count = 0;
+};
+WsLayout ws_layout(int d);
+int launch_centroids(const float* E32, int d, const int64_t* col_ptr,
+                     const uint2* ent, int64_t N, float* C, cudaStream_t st);
+int launch_solve_f64(const float* K, int ld, int vr, const double* r,
+                     const int64_t* col_ptr, const uint2* ent, const int32_t* docs,
+                     int ndocs, double tol, int cap, double* u_out, int* it_out,
+                     double* res_out, cudaStream_t st);
+int launch_ws_rows(const float* E32, int d, const float* C, const float* K, int ld,
+                   float expo, const uint32_t* src_ids, const double* r, int vr,
+                   const int64_t* col_ptr, const uint2* ent, const int32_t* docs,
+                   const double* u, int ndocs, const int32_t* sel, int G,
+                   const int64_t* row0, int F, float* X, float* y, cudaStream_t st);
+int launch_ws_colstats(const float* X, int64_t P, int F, double* s1, double* s2,
+                       int chunks, cudaStream_t st);
+int launch_ws_standardize(float* X, int64_t P, int F, const float* shift,
+                          const float* scale, cudaStream_t st);
+size_t ws_scratch_floats(int64_t P, int F);
+int launch_ws_fwd_bwd(const WsLayout& L, const float* params, const float* X,
+                      const float* t, const int64_t* gptr, int64_t ngroups,
+                      int64_t P, float* grad, double* loss_g, float* scratch,
+                      cudaStream_t st);
+int launch_ws_adam(const WsLayout& L, float* params, const float* grad, float* m1,
+                   float* m2, float lr, int step, cudaStream_t st);
+int launch_ws_gather(const float* X, const float* t, const int64_t* gptr,
+                     const int64_t* perm, const int64_t* bptr, int64_t g0, int64_t ng,
+                     int F, float* Xb, float* tb, cudaStream_t st);
+size_t ws_folded_floats(const WsLayout& L);
+int launch_ws_fold(const WsLayout& L, const float* params, float* folded,
+                   cudaStream_t st);
+int launch_ws_doc_bias(const WsLayout& L, const float* folded, const float* C,
+                       int64_t N, float* Bdoc, cudaStream_t st);
+int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
+                   const float* S, const float* rinv, int vr, const float* K, int ld,
+                   float expo, const Targets& t, const float* Bdoc, float* Asrc,
+                   float* u0, int64_t ldu, unsigned* err, int num_sms,
+                   cudaStream_t st);
 
 }  // namespace wmd
