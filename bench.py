@@ -57,6 +57,14 @@ def args_():
     ap.add_argument("--cdist", choices=["fp32", "fp16", "bf16"], default="fp32",
                     help="cost-panel precision: fp32 CUDA cores (plain form) or "
                          "tcgen05 tensor cores with 16-bit operands")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the precision-form, converged and batched / "
+                         "warm-start sections (single GPU only)")
+    ap.add_argument("--batch-sources", type=int, default=128,
+                    help="sources of the 512-source batched workload timed")
+    ap.add_argument("--no-warm-start", action="store_true")
+    ap.add_argument("--ws-train-sources", type=int, default=128,
+                    help="training sources of the warm-start model")
     return ap.parse_args()
 
 
@@ -246,6 +254,139 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
+# Extra sections (one GPU): precision form, converged criterion, batched
+# queries with the BF16 panel and the learned warm start.
+# ---------------------------------------------------------------------------
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    e = np.abs(a - b) / np.abs(b)
+    e[np.isnan(a) & np.isnan(b)] = 0.0
+    return e
+
+
+def extras(a, wmd, p, dev):
+    import torch
+    import oracle
+    synth = importlib.import_module(PKG + ".synth")
+    W = WORKLOAD
+    out = {}
+    sub = 200
+    cp = p.col_ptr[:sub + 1]
+    args = (p.vecs.astype(np.float64), cp, p.row_inds[:cp[-1]], p.vals[:cp[-1]])
+    ref15 = oracle.sinkhorn(p.r, *args, p.lam, p.max_iter)
+    conv, conv_it, _, _ = oracle.sinkhorn_converged(p.r, *args, p.lam, tol=1e-9,
+                                                    max_iter_cap=50000)
+
+    def timed(eng, fn, reps):
+        fn()
+        eng.check()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        eng.check()
+        return (time.perf_counter() - t0) / reps
+
+    # 1. the two single-source forms of the same workload
+    eng = wmd.Engine(dev.index)
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    r_dev = torch.from_numpy(p.r).to(dev)
+    o = torch.empty(p.N, dtype=torch.float64, device=dev)
+    forms = {}
+    for mode in ("fp32", "fp16", "bf16"):
+        eng.set_cdist_mode(mode)
+        fn = lambda: eng.query_device(r_dev.data_ptr(), W["v_r"], p.lam, p.max_iter,
+                                      o.data_ptr())
+        dt = timed(eng, fn, 50)
+        got = o[:sub].cpu().numpy()
+        e15, ec = _rel(got, ref15), _rel(got, conv)
+        forms[mode] = {"pairs_per_s": p.N / dt,
+                       "rel_err_vs_fp64_15it": {"max": float(e15.max()),
+                                                "median": float(np.median(e15))},
+                       "rel_err_vs_converged_fp64": {"max": float(ec.max()),
+                                                     "median": float(np.median(ec))}}
+    out["single_source_forms"] = forms
+    # 2. converged criterion: marginal residual <= 1e-4 per document (WMD
+    #    within ~6e-5 of the converged FP64 oracle), cap 5000 updates
+    eng.set_cdist_mode("fp32")
+    eng.set_tolerance(1e-4)
+    fn = lambda: eng.query_device(r_dev.data_ptr(), W["v_r"], p.lam, 5000, o.data_ptr())
+    dt = timed(eng, fn, 20)
+    it = eng.last_iterations()
+    ec = _rel(o[:sub].cpu().numpy(), conv)
+    out["single_source_converged"] = {
+        "tol_marginal_residual": 1e-4, "pairs_per_s": p.N / dt,
+        "iters_mean": float(it.mean()), "iters_max": int(it.max()),
+        "rel_err_vs_converged_fp64_max": float(ec.max()),
+        "oracle_iters_to_1e-9_mean": float(conv_it.mean())}
+    eng.close()
+
+    # 3. batched queries: sources of the 512-source set (v_r ~ U[4,512])
+    #    against N = 100000 targets
+    V, d, N = W["V"], W["d"], 100_000
+    cdf = synth.zipf_cdf(V)
+    cpb, rib, vab = synth.targets(V, N, 8, 256, seed=2, cdf=cdf)
+    rs, vrs = synth.batched_sources(V, 512, 4, 512, seed=7, cdf=cdf)
+    S = min(a.batch_sources, 512)
+    rs, vrs = rs[:S], vrs[:S]
+    eng = wmd.Engine(dev.index)
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(cpb, rib, vab)
+    batched = {"sources": S, "sum_vr": int(sum(vrs)), "docs": N,
+               "nnz": int(cpb[-1])}
+    for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
+        eng.set_solve_precision(prec)
+        eng.query_batch(rs[:2], p.lam, 15)
+        t0 = time.perf_counter()
+        res = eng.query_batch(rs, p.lam, 15)
+        dt = time.perf_counter() - t0
+        batched[name] = {"pairs_per_s": S * N / dt, "seconds": dt, "iters": 15}
+        if prec == "fp32":
+            res_fp32 = res
+    e = _rel(res, res_fp32)
+    batched["bf16_panel"]["max_rel_diff_vs_fp32_panel"] = float(np.nanmax(e))
+    # converged (residual <= 1e-4): cold start vs the learned warm start on
+    # held-out sources
+    rng = np.random.default_rng(11)
+    held = [synth.source_doc(V, int(v), seed=5000 + q, cdf=cdf)
+            for q, v in enumerate(rng.integers(4, 513, 16))]
+    eng.set_solve_precision("bf16")
+    eng.set_tolerance(1e-4)
+    t0 = time.perf_counter()
+    cold, itc = eng.query_batch(held, p.lam, 5000, want_iters=True)
+    tc = time.perf_counter() - t0
+    conv_b = {"sources": len(held), "tol_marginal_residual": 1e-4,
+              "cold": {"pairs_per_s": len(held) * N / tc,
+                       "iters_mean": float(itc.mean())}}
+    if not a.no_warm_start:
+        train = [synth.source_doc(V, int(v), seed=1000 + q, cdf=cdf)
+                 for q, v in enumerate(rng.integers(4, 513, a.ws_train_sources))]
+        t0 = time.perf_counter()
+        info = eng.ws_build_training_set(train, p.lam, docs_per_source=40,
+                                         words_per_doc=16, label_tol=1e-7,
+                                         label_max_iter=3000, seed=1)
+        t_lab = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        params, loss = eng.ws_train(wmd.ws_init_params(d, 0), epochs=60,
+                                    batch_groups=256, lr=3e-3)
+        t_tr = time.perf_counter() - t0
+        eng.set_warm_start(params)
+        t0 = time.perf_counter()
+        warm, itw = eng.query_batch(held, p.lam, 5000, want_iters=True)
+        tw = time.perf_counter() - t0
+        conv_b["warm"] = {"pairs_per_s": len(held) * N / tw,
+                          "iters_mean": float(itw.mean()),
+                          "max_rel_diff_vs_cold": float(np.nanmax(_rel(warm, cold))),
+                          "training": {"rows": info["rows"], "pairs": info["groups"],
+                                       "label_seconds": t_lab, "train_seconds": t_tr,
+                                       "final_loss": float(loss[-1])}}
+    batched["converged"] = conv_b
+    out["batched"] = batched
+    eng.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Our arm.
 # ---------------------------------------------------------------------------
 def ours(a, rank, world, local):
@@ -403,6 +544,12 @@ def ours(a, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(p, a.cpu_seconds)
+    extra = None
+    if rank == 0 and world == 1 and not a.no_extras:
+        try:
+            extra = extras(a, wmd, p, dev)
+        except Exception as exc:  # reported, never fatal to the main line
+            extra = {"error": f"{type(exc).__name__}: {exc}"}
 
     if rank == 0:
         line = {
@@ -433,6 +580,7 @@ def ours(a, rank, world, local):
             "max_rel_err_vs_oracle": max_rel,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "extras": extra,
             "clocks": clocks,
             "wall_s_timed_region": wall,
         }
