@@ -329,6 +329,36 @@ wmd_status wmd_set_warm_start(wmd_handle* h, const float* params);
 wmd_status wmd_ws_init_scalings(wmd_handle* h, const double* r, double lambda,
                                 float* u0_out, uint64_t* vr_out);
 
+/* ---------------------------------------------------------------------------
+ * The reference's input files and edge lists.
+ * ------------------------------------------------------------------------ */
+/* mat.mtx (sinkhorn_wmd_fused.cpp:427-486): header "num_rows num_cols nnz",
+ * then nnz triples "word doc weight", 1-based.  wmd_read_mtx writes 0-based
+ * word and document ids and the weights in file order (arrays of nnz_cap >=
+ * the header's nnz); invalid entries (id 0 or out of range, weight <= 0,
+ * missing triples) return WMD_ERR_INVALID_INPUT, as the reference exits. */
+wmd_status wmd_mtx_header(const char* path, uint64_t* num_rows, uint64_t* num_cols,
+                          uint64_t* nnz);
+wmd_status wmd_read_mtx(const char* path, uint64_t nnz_cap, uint64_t* words,
+                        uint64_t* docs, double* weights, uint64_t* nnz_out);
+/* vecs.out (:511-549): V lines of d space-separated values -> vecs[V*d]. */
+wmd_status wmd_read_vecs(const char* path, uint64_t V, uint64_t d, double* vecs);
+/* r.out (:552-586): V whitespace-separated values >= 0 -> r[V]. */
+wmd_status wmd_read_r(const char* path, uint64_t V, double* r);
+/* Edge list (0-based, any order) -> document-major CSC built on the GPU:
+ * entries sorted by (document, word, edge index), i.e. exactly the
+ * reference's stable counting sort into CSR (:493-506) followed by a stable
+ * transpose.  wmd_edges_to_csc returns it to host arrays (col_ptr[N+1],
+ * rows[nnz], vals[nnz]); wmd_set_targets_edges makes it the handle's
+ * target set. */
+wmd_status wmd_edges_to_csc(wmd_handle* h, const uint64_t* words, const uint64_t* docs,
+                            const double* w, uint64_t nnz, uint64_t V, uint64_t N,
+                            uint64_t* col_ptr_out, uint64_t* rows_out,
+                            double* vals_out);
+wmd_status wmd_set_targets_edges(wmd_handle* h, const uint64_t* words,
+                                 const uint64_t* docs, const double* w, uint64_t nnz,
+                                 uint64_t V, uint64_t N);
+
 #ifdef __cplusplus
 }
 #endif

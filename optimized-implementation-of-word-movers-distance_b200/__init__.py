@@ -153,6 +153,36 @@ def ws_init_params(d: int, seed: int = 0) -> np.ndarray:
     return p
 
 
+def read_mtx(path):
+    """The reference's mat.mtx: (V, N, words, docs, weights), 0-based ids in
+    file order."""
+    V, N, Z = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    b = str(path).encode()
+    check(lib().wmd_mtx_header(b, ctypes.byref(V), ctypes.byref(N), ctypes.byref(Z)))
+    words = np.empty(Z.value, np.uint64)
+    docs = np.empty(Z.value, np.uint64)
+    w = np.empty(Z.value, np.float64)
+    n = ctypes.c_uint64()
+    check(lib().wmd_read_mtx(b, Z.value, _ptr(words, ctypes.c_uint64),
+                             _ptr(docs, ctypes.c_uint64), _ptr(w, ctypes.c_double),
+                             ctypes.byref(n)))
+    return V.value, N.value, words, docs, w
+
+
+def read_vecs(path, V: int, d: int) -> np.ndarray:
+    """The reference's vecs.out: (V, d) float64."""
+    out = np.empty((V, d), np.float64)
+    check(lib().wmd_read_vecs(str(path).encode(), V, d, _ptr(out, ctypes.c_double)))
+    return out
+
+
+def read_r(path, V: int) -> np.ndarray:
+    """The reference's r.out: V non-negative values."""
+    out = np.empty(V, np.float64)
+    check(lib().wmd_read_r(str(path).encode(), V, _ptr(out, ctypes.c_double)))
+    return out
+
+
 class Engine:
     """Resident-corpus solver (handle API of include/wmd_b200.h).  ``lam`` is
     the positive regulariser: K = exp(-lam * M)."""
@@ -222,6 +252,27 @@ class Engine:
         V = row_ptr.size - 1
         s, _keep = _csr_struct(V, int(N), row_ptr, col_inds, vals)
         check(lib().wmd_set_targets_csr(self._h, ctypes.byref(s)))
+        self.N = int(N)
+
+    def edges_to_csc(self, words, docs, w, V: int, N: int):
+        """GPU CSC build of an edge list: (col_ptr, rows, vals)."""
+        words, docs, w = _u64(words), _u64(docs), _f64(w)
+        cp = np.empty(N + 1, np.uint64)
+        rows = np.empty(words.size, np.uint64)
+        vals = np.empty(words.size, np.float64)
+        check(lib().wmd_edges_to_csc(
+            self._h, _ptr(words, ctypes.c_uint64), _ptr(docs, ctypes.c_uint64),
+            _ptr(w, ctypes.c_double), words.size, int(V), int(N),
+            _ptr(cp, ctypes.c_uint64), _ptr(rows, ctypes.c_uint64),
+            _ptr(vals, ctypes.c_double)))
+        return cp, rows, vals
+
+    def set_targets_edges(self, words, docs, w, V: int, N: int):
+        """Target set from an edge list (e.g. read_mtx), CSC built on the GPU."""
+        words, docs, w = _u64(words), _u64(docs), _f64(w)
+        check(lib().wmd_set_targets_edges(
+            self._h, _ptr(words, ctypes.c_uint64), _ptr(docs, ctypes.c_uint64),
+            _ptr(w, ctypes.c_double), words.size, int(V), int(N)))
         self.N = int(N)
 
     def set_cdist_mode(self, mode: str):

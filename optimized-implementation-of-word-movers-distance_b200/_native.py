@@ -85,6 +85,17 @@ _SIGS = [
      [ctypes.c_void_p, c_f32p, c_f32p, c_i64p, ctypes.POINTER(ctypes.c_uint32),
       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_int32)]),
     ("wmd_set_warm_start", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
+    ("wmd_mtx_header", ctypes.c_int, [ctypes.c_char_p, c_u64p, c_u64p, c_u64p]),
+    ("wmd_read_mtx", ctypes.c_int,
+     [ctypes.c_char_p, ctypes.c_uint64, c_u64p, c_u64p, c_f64p, c_u64p]),
+    ("wmd_read_vecs", ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, c_f64p]),
+    ("wmd_read_r", ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, c_f64p]),
+    ("wmd_edges_to_csc", ctypes.c_int,
+     [ctypes.c_void_p, c_u64p, c_u64p, c_f64p, ctypes.c_uint64, ctypes.c_uint64,
+      ctypes.c_uint64, c_u64p, c_u64p, c_f64p]),
+    ("wmd_set_targets_edges", ctypes.c_int,
+     [ctypes.c_void_p, c_u64p, c_u64p, c_f64p, ctypes.c_uint64, ctypes.c_uint64,
+      ctypes.c_uint64]),
     ("wmd_ws_init_scalings", ctypes.c_int,
      [ctypes.c_void_p, c_f64p, ctypes.c_double, c_f32p, c_u64p]),
     ("wmd_query_dense", ctypes.c_int,

@@ -76,6 +76,7 @@ std::string describe_err_bits(unsigned bits) {
   if (bits & ERR_BAD_VAL) s += " target value <= 0 or not finite;";
   if (bits & ERR_VR_CAP) s += " more non-zero source words than vr_cap;";
   if (bits & ERR_TIMEOUT) s += " device-side wait timed out (kernel aborted);";
+  if (bits & ERR_DOC_RANGE) s += " document index >= number of documents;";
   return s;
 }
 
@@ -122,6 +123,7 @@ struct wmd_handle {
   int e16_fmt = -1;  // format E16 holds (1 bf16, 2 fp16), -1 = stale
   // targets
   DevBuf col_ptr, ent, order, stage_cp, stage_rows, stage_vals;
+  DevBuf edge_words, edge_docs, edge_w, edge_temp;  // edge-list CSC build
   uint64_t tV = 0, N = 0, nnz = 0;
   bool have_T = false;
   // per query
@@ -914,7 +916,8 @@ wmd_status wmd_destroy(wmd_handle* h) {
                     &h->b_rinv, &h->b_vr, &h->b_out, &h->b_iters,
                     &h->topk_scratch, &h->topk_idx, &h->topk_val, &h->K16,
                     &h->ws_params, &h->ws_folded, &h->ws_C, &h->ws_Bdoc,
-                    &h->ws_Asrc, &h->ws_u0, &h->ws_X, &h->ws_y, &h->ws_gptr})
+                    &h->ws_Asrc, &h->ws_u0, &h->ws_X, &h->ws_y, &h->ws_gptr,
+                    &h->edge_words, &h->edge_docs, &h->edge_w, &h->edge_temp})
     b->release();
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->chunks_host) cudaFreeHost(h->chunks_host);
@@ -1532,6 +1535,92 @@ wmd_status wmd_ws_init_scalings(wmd_handle* h, const double* r, double lambda,
   if (vr == 0) return WMD_OK;
   CK(cudaMemcpy2D(u0_out, vr * sizeof(float), h->ws_u0.p, ld * sizeof(float),
                   vr * sizeof(float), h->N, cudaMemcpyDeviceToHost));
+  return WMD_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * Edge lists (the reference's mat.mtx entries) -> document-major CSC on the
+ * GPU.
+ * ---------------------------------------------------------------------- */
+static wmd_status edges_to_stage(wmd_handle* h, const uint64_t* words,
+                                 const uint64_t* docs, const double* w, uint64_t nnz,
+                                 uint64_t V, uint64_t N) {
+  if (!h || (nnz && (!words || !docs || !w)) || V == 0 || N == 0)
+    return fail(WMD_ERR_INVALID_ARG, "bad argument");
+  if (nnz == 0) return fail(WMD_ERR_INVALID_INPUT, "edge list is empty");
+  if (N >= 0x7FFFFFFFull) return fail(WMD_ERR_UNSUPPORTED, "more than 2^31-1 documents");
+  wmd_status st = bind(h);
+  if (st) return st;
+  const size_t tb = csc_build_temp_bytes(nnz, V, N);
+  CK(h->edge_words.ensure(nnz * 8));
+  CK(h->edge_docs.ensure(nnz * 8));
+  CK(h->edge_w.ensure(nnz * 8));
+  CK(h->edge_temp.ensure(tb));
+  CK(h->stage_cp.ensure((N + 1) * 8));
+  CK(h->stage_rows.ensure(nnz * 8));
+  CK(h->stage_vals.ensure(nnz * 8));
+  CK(cudaMemcpyAsync(h->edge_words.p, words, nnz * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->edge_docs.p, docs, nnz * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->edge_w.p, w, nnz * 8, cudaMemcpyHostToDevice, h->stream));
+  st = clear_err(h);
+  if (st) return st;
+  const int n = launch_csc_build(h->edge_words.as<uint64_t>(), h->edge_docs.as<uint64_t>(),
+                                 h->edge_w.as<double>(), nnz, V, N, h->edge_temp.p, tb,
+                                 h->stage_cp.as<uint64_t>(), h->stage_rows.as<uint64_t>(),
+                                 h->stage_vals.as<double>(), h->err_dev.as<unsigned>(),
+                                 h->stream);
+  if (n < 0) return fail(WMD_ERR_UNSUPPORTED, "edge list too large for the GPU sort");
+  CK(cudaGetLastError());
+  h->last_launches = n;
+  return finish(h);
+}
+
+wmd_status wmd_edges_to_csc(wmd_handle* h, const uint64_t* words, const uint64_t* docs,
+                            const double* w, uint64_t nnz, uint64_t V, uint64_t N,
+                            uint64_t* col_ptr_out, uint64_t* rows_out,
+                            double* vals_out) {
+  if (!col_ptr_out || !rows_out || !vals_out) return fail(WMD_ERR_INVALID_ARG, "null output");
+  wmd_status st = edges_to_stage(h, words, docs, w, nnz, V, N);
+  if (st) return st;
+  CK(cudaMemcpy(col_ptr_out, h->stage_cp.p, (N + 1) * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(rows_out, h->stage_rows.p, nnz * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(vals_out, h->stage_vals.p, nnz * 8, cudaMemcpyDeviceToHost));
+  return WMD_OK;
+}
+
+wmd_status wmd_set_targets_edges(wmd_handle* h, const uint64_t* words,
+                                 const uint64_t* docs, const double* w, uint64_t nnz,
+                                 uint64_t V, uint64_t N) {
+  wmd_status st = edges_to_stage(h, words, docs, w, nnz, V, N);
+  if (st) return st;
+  std::vector<uint64_t> cp(N + 1);
+  CK(cudaMemcpy(cp.data(), h->stage_cp.p, (N + 1) * 8, cudaMemcpyDeviceToHost));
+  std::vector<int32_t> ord;
+  length_order(cp.data(), N, ord);
+  CK(h->col_ptr.ensure((N + 1) * sizeof(int64_t)));
+  CK(h->ent.ensure(nnz * sizeof(uint2)));
+  CK(h->order.ensure(N * sizeof(int32_t)));
+  CK(cudaMemcpyAsync(h->order.p, ord.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice,
+                     h->stream));
+  st = clear_err(h);
+  if (st) return st;
+  const int launches = launch_pack_targets(
+      h->stage_cp.as<uint64_t>(), h->stage_rows.as<uint64_t>(), h->stage_vals.as<double>(),
+      V, N, nnz, h->col_ptr.as<int64_t>(), h->ent.as<uint2>(), h->err_dev.as<unsigned>(),
+      h->stream);
+  CK(cudaGetLastError());
+  h->have_T = false;
+  st = finish(h);
+  if (st) return st;
+  h->tV = V;
+  h->N = N;
+  h->nnz = nnz;
+  h->have_T = true;
+  h->ws_docs_ready = false;
+  h->doc_len.resize(N);
+  for (uint64_t j = 0; j < N; ++j) h->doc_len[j] = (uint32_t)(cp[j + 1] - cp[j]);
+  h->graph_epoch++;
+  h->last_launches += launches;
   return WMD_OK;
 }
 

@@ -27,6 +27,7 @@ enum : unsigned {
   ERR_BAD_VAL = 8u,    // target value <= 0 or not finite
   ERR_VR_CAP = 16u,    // more selected source words than the panel capacity
   ERR_TIMEOUT = 32u,   // a bounded device-side wait gave up (kernel aborted)
+  ERR_DOC_RANGE = 64u, // document id >= N (edge-list input)
 };
 
 constexpr int kSelectThreads = 256;
@@ -236,5 +237,15 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
                    float expo, const Targets& t, const float* Bdoc, float* Asrc,
                    float* u0, int64_t ldu, unsigned* err, int num_sms,
                    cudaStream_t st);
+
+// GPU CSC build from an edge list (csc_build.cu).  The result equals the
+// host's stable counting sorts word-major (file order within a word,
+// sinkhorn_wmd_fused.cpp:493-506) then document-major: entries sorted by
+// (document, word, edge index).
+size_t csc_build_temp_bytes(uint64_t nnz, uint64_t V, uint64_t N);
+int launch_csc_build(const uint64_t* words, const uint64_t* docs, const double* w,
+                     uint64_t nnz, uint64_t V, uint64_t N, void* temp,
+                     size_t temp_bytes, uint64_t* col_ptr, uint64_t* rows,
+                     double* vals, unsigned* err, cudaStream_t st);
 
 }  // namespace wmd
