@@ -345,6 +345,9 @@ def extras(a, wmd, p, dev):
             res_fp32 = res
     e = _rel(res, res_fp32)
     batched["bf16_panel"]["max_rel_diff_vs_fp32_panel"] = float(np.nanmax(e))
+    batched["bf16_panel"]["autotuned_shapes"] = {
+        f"ld16={k[0]}{' beyond 64MiB' if k[1] else ''}": v
+        for k, v in eng.autotune_choices().items()}
     # converged (residual <= 1e-4): cold start vs the learned warm start on
     # held-out sources
     rng = np.random.default_rng(11)

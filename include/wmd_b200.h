@@ -154,6 +154,16 @@ typedef enum wmd_solve_precision {
 } wmd_solve_precision;
 wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec);
 
+/* Launch-shape autotuner of the BF16 block solve (on by default): the first
+ * solve of each panel width (and panel size class: within / beyond 64 MiB)
+ * times every candidate shape on the handle's real data and keeps the
+ * fastest.  wmd_autotune_choices fills shapes[8] (index (width/128 - 1) * 2 +
+ * beyond; -2 = not tuned yet, -1 = build-time default); the name of a shape
+ * comes from wmd_block_shape_name. */
+wmd_status wmd_set_autotune(wmd_handle* h, int enable);
+wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes);
+const char* wmd_block_shape_name(int shape);
+
 /* One source document as a dense host histogram r[V] (the reference's form,
  * zeros skipped as sinkhorn_wmd_fused.cpp:45-63 does).  wmd_out: host, N. */
 wmd_status wmd_query_dense(wmd_handle* h, const double* r, double lambda,

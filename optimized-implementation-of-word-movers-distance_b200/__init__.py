@@ -278,6 +278,19 @@ class Engine:
     def set_cdist_mode(self, mode: str):
         check(lib().wmd_set_cdist_mode(self._h, CDIST_MODES[mode]))
 
+    def set_autotune(self, enable: bool = True):
+        check(lib().wmd_set_autotune(self._h, int(bool(enable))))
+
+    def autotune_choices(self) -> dict:
+        """{(panel width, beyond 64 MiB): chosen block-solve launch shape}."""
+        a = (ctypes.c_int * 8)()
+        check(lib().wmd_autotune_choices(self._h, a))
+        out = {}
+        for i, v in enumerate(a):
+            if v != -2:
+                out[(128 * (i // 2 + 1), bool(i % 2))] = lib().wmd_block_shape_name(v).decode()
+        return out
+
     def set_solve_precision(self, prec: str):
         """'fp32' (default) or 'bf16': K panel storage read by the iterations
         for sources with 64 < v_r <= 512."""

@@ -69,6 +69,9 @@ _SIGS = [
     ("wmd_set_targets_csr", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSR)]),
     ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_solve_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_autotune_choices", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    ("wmd_block_shape_name", ctypes.c_char_p, [ctypes.c_int]),
     ("wmd_ws_param_count", ctypes.c_uint64, [ctypes.c_uint64]),
     ("wmd_ws_init_params", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, c_f32p]),
     ("wmd_ws_build_training_set", ctypes.c_int,

@@ -116,6 +116,10 @@ struct wmd_handle {
   // Storage of the K panel the solve reads for 64 < v_r <= 512 (BF16: the
   // CTA-per-document kernel with the rows staged in shared memory).
   wmd_solve_precision prec = WMD_SOLVE_FP32;
+  // Launch-shape autotuner of the block solve: per (panel width, panel
+  // beyond L2) the fastest shape measured on this handle's data.
+  bool autotune = true;
+  int blk_shape[8] = {-2, -2, -2, -2, -2, -2, -2, -2};  // -2: not tuned yet
   // embeddings
   DevBuf E32, nE, E64_stage, E16;
   uint64_t V = 0, d = 0;
@@ -226,6 +230,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
   h->have_E = true;
   h->e16_fmt = -1;
   h->ws_docs_ready = false;
+  for (int& x : h->blk_shape) x = -2;
   h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
@@ -297,6 +302,7 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   h->nnz = nnz;
   h->have_T = true;
   h->ws_docs_ready = false;
+  for (int& x : h->blk_shape) x = -2;
   h->doc_len.resize(N);
   for (uint64_t j = 0; j < N; ++j) h->doc_len[j] = (uint32_t)(c->col_ptr[j + 1] - c->col_ptr[j]);
   h->graph_epoch++;
@@ -336,6 +342,48 @@ wmd_status csr_to_csc_host(const wmd_csr_double_t* a, std::vector<uint64_t>& cp,
       vals[pos] = a->vals[e];
     }
   return WMD_OK;
+}
+
+// Launch shape of the block solve for this panel: cached per (width, panel
+// beyond L2); when not yet known and the call may synchronise, every
+// candidate shape is timed on the real panel and target set (4 updates, CUDA
+// events) and the fastest is kept.  Returns -1 (build-time default) when
+// tuning is off or impossible (inside a graph capture).
+int block_shape_for(wmd_handle* h, const void* K16, int ld16, float expo,
+                    uint32_t vr, const SourceSel& sel, const Targets& t,
+                    const SolveCtl& ctl, double* out, bool can_sync) {
+  const int key = ((ld16 / 128 - 1) & 3) * 2 + ((size_t)h->V * ld16 * 2 > (64u << 20) ? 1 : 0);
+  if (h->blk_shape[key] != -2) return h->blk_shape[key];
+  if (!h->autotune || !can_sync) return -1;
+  SolveCtl c2 = ctl;
+  c2.max_iter = 4;
+  c2.tol = 0.f;
+  c2.iters = nullptr;
+  c2.u0 = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    if (a) cudaEventDestroy(a);
+    return -1;
+  }
+  float best = 1e30f;
+  int bi = -1;
+  for (int sh = 0; sh < block_shape_count(); ++sh) {
+    if (launch_solve_block(K16, ld16, expo, vr, sel, t, c2, nullptr, 0, out, h->stream, sh) < 0)
+      continue;  // shape unavailable (shared-memory budget)
+    cudaEventRecord(a, h->stream);
+    launch_solve_block(K16, ld16, expo, vr, sel, t, c2, nullptr, 0, out, h->stream, sh);
+    cudaEventRecord(b, h->stream);
+    float ms = 0.f;
+    if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess &&
+        ms < best) {
+      best = ms;
+      bi = sh;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  h->blk_shape[key] = bi;
+  return bi;
 }
 
 // Warm start: target centroids and the per-document first-layer terms of the
@@ -473,8 +521,10 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     if (ld16) {
       n += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V, sel.vr,
                                 h->sms, h->stream);
+      const int shape = block_shape_for(h, h->K16.p, ld16, expo, cap, sel, t, ctl,
+                                        out_dev, !capturing);
       const int ls = launch_solve_block(h->K16.p, ld16, expo, cap, sel, t, ctl,
-                                        ctl.u0, ctl.ldu, out_dev, h->stream);
+                                        ctl.u0, ctl.ldu, out_dev, h->stream, shape);
       if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "block solve unavailable");
       n += ls;
     } else {
@@ -763,8 +813,10 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     if (ld16) {
       launches += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V,
                                        sel.vr, h->sms, h->stream);
+      const int shape = block_shape_for(h, h->K16.p, ld16, expo, vr, sel, t, ctl,
+                                        h->b_out.as<double>() + s * N, true);
       ls = launch_solve_block(h->K16.p, ld16, expo, vr, sel, t, ctl, ctl.u0, ctl.ldu,
-                              h->b_out.as<double>() + s * N, h->stream);
+                              h->b_out.as<double>() + s * N, h->stream, shape);
     } else {
       ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
                         h->b_out.as<double>() + s * N, h->stream);
@@ -968,6 +1020,22 @@ wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
   h->mode = mode;
   return WMD_OK;
 }
+
+wmd_status wmd_set_autotune(wmd_handle* h, int enable) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  h->autotune = enable != 0;
+  for (int& x : h->blk_shape) x = -2;
+  h->graph_epoch++;
+  return WMD_OK;
+}
+
+wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes) {
+  if (!h || !shapes) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  for (int i = 0; i < 8; ++i) shapes[i] = h->blk_shape[i];
+  return WMD_OK;
+}
+
+const char* wmd_block_shape_name(int shape) { return block_shape_name(shape); }
 
 wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
@@ -1617,6 +1685,7 @@ wmd_status wmd_set_targets_edges(wmd_handle* h, const uint64_t* words,
   h->nnz = nnz;
   h->have_T = true;
   h->ws_docs_ready = false;
+  for (int& x : h->blk_shape) x = -2;
   h->doc_len.resize(N);
   for (uint64_t j = 0; j < N; ++j) h->doc_len[j] = (uint32_t)(cp[j + 1] - cp[j]);
   h->graph_epoch++;

@@ -6,7 +6,7 @@
 // fused solver uses for K and K_over_r (sinkhorn_wmd_fused.cpp:197-223), so a
 // target document's gather of one word is one contiguous ld-float row.
 //
-// M comes from the GEMM form ||E_w||^2 + ||S_i||^2 - 2 E_w.S_i (a 128 x 32
+// M comes from the GEMM form ||E_w||^2 + ||S_i||^2 - 2 E_w.S_i (a BM x 32
 // register-tiled SIMT GEMM over d).  That form cancels catastrophically for
 // close pairs (a word against itself gives M ~ 1e-3 instead of 0, i.e. a 1%
 // error in K at lambda = 10), so pairs whose GEMM-form M^2 falls below
@@ -19,17 +19,30 @@
 
 namespace wmd {
 
+// Rows per thread (tile height BM = 16 * RPT) and resident CTAs per SM: a
+// build-time tuning knob.
+#ifndef WMD_CDIST_RPT
+#define WMD_CDIST_RPT 8
+#endif
+#ifndef WMD_CDIST_MINB
+#define WMD_CDIST_MINB 1
+#endif
+
 namespace {
-constexpr int BM = 128;        // vocabulary rows per CTA
+constexpr int RPT = WMD_CDIST_RPT;
+constexpr int BM = 16 * RPT;   // vocabulary rows per CTA
 constexpr int BN = 32;         // source words per CTA
 constexpr int BK = 16;         // d-slice per stage
-constexpr int THREADS = 128;   // 16 x 8 threads, each 8 rows x 4 sources
+constexpr int THREADS = 128;   // 16 x 8 threads, each RPT rows x 4 sources
 constexpr int AS = BM + 4;     // padded smem row (floats)
+constexpr int ALOADS = BM * BK / 4 / THREADS;  // float4 A slots per thread
+static_assert(RPT % 4 == 0 || RPT == 6 || RPT == 2, "RPT");
+static_assert(BM * BK / 4 == ALOADS * THREADS, "A tile load split");
 
 }  // namespace
 
 template <bool VEC4>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, WMD_CDIST_MINB)
 cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
                   uint64_t V, int d, const float* __restrict__ S,
                   const float* __restrict__ nS,
@@ -44,20 +57,20 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
   const int n0 = blockIdx.y * BN;
   const int vr = (int)*vr_dev;
 
-  float acc[8][4];
+  float acc[RPT][4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < RPT; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
 
   const bool active = n0 < vr;  // tiles of pure padding only write zeros
   if (active) {
-    float4 ra[4];
+    float4 ra[ALOADS];
     float4 rb;
     auto load_tile = [&](int k0) {
 #pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        const int f = tid + p * THREADS;  // 512 float4 slots: 128 rows x 4
+      for (int p = 0; p < ALOADS; ++p) {
+        const int f = tid + p * THREADS;  // BM rows x 4 float4 slots
         const int row = f >> 2, kq = f & 3;
         const uint64_t gr = m0 + row;
         const int k = k0 + kq * 4;
@@ -96,7 +109,7 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
     };
     auto store_tile = [&](int buf) {
 #pragma unroll
-      for (int p = 0; p < 4; ++p) {
+      for (int p = 0; p < ALOADS; ++p) {
         const int f = tid + p * THREADS;
         const int row = f >> 2, kq = f & 3;
         As[buf][kq * 4 + 0][row] = ra[p].x;
@@ -120,13 +133,28 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
       if (kt + 1 < nk) load_tile((kt + 1) * BK);
 #pragma unroll
       for (int k = 0; k < BK; ++k) {
-        const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][k][ty * 8]);
-        const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][k][ty * 8 + 4]);
+        float av[RPT];
+        if constexpr (RPT % 4 == 0) {
+#pragma unroll
+          for (int i = 0; i < RPT; i += 4) {
+            const float4 a = *reinterpret_cast<const float4*>(&As[buf][k][ty * RPT + i]);
+            av[i] = a.x;
+            av[i + 1] = a.y;
+            av[i + 2] = a.z;
+            av[i + 3] = a.w;
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < RPT; i += 2) {
+            const float2 a = *reinterpret_cast<const float2*>(&As[buf][k][ty * RPT + i]);
+            av[i] = a.x;
+            av[i + 1] = a.y;
+          }
+        }
         const float4 b = *reinterpret_cast<const float4*>(&Bs[buf][k][tx * 4]);
-        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
         const float bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < RPT; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
       }
@@ -142,8 +170,8 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
   const int c0 = n0 + tx * 4;
   if (c0 >= ld) return;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const uint64_t w = m0 + ty * 8 + i;
+  for (int i = 0; i < RPT; ++i) {
+    const uint64_t w = m0 + ty * RPT + i;
     if (w >= V) break;
     const float ne = active ? nE[w] : 0.f;
     float kv[4], kmv[4];

@@ -414,16 +414,38 @@ static int launch_block_t(const void* K16, int ld16, float expo,
   return 1;
 }
 
+// Launch shapes the autotuner chooses from (warps per CTA, CTAs per SM).
+// shape < 0 selects the build-time table above.
+int block_shape_count() { return 3; }
+const char* block_shape_name(int shape) {
+  static const char* names[] = {"4 warps x 4 CTAs/SM", "8 warps x 2 CTAs/SM",
+                                "16 warps x 1 CTA/SM"};
+  return shape >= 0 && shape < 3 ? names[shape] : "build-time table";
+}
+
+template <int NQ, int W, int C>
+static int launch_nq_default(const void* K16, int ld16, float expo, const SourceSel& s,
+                             const Targets& t, const SolveCtl& ctl, const float* u0,
+                             int64_t ldu, double* out, cudaStream_t st, int shape) {
+  switch (shape) {
+    case 0: return launch_block_t<NQ, 4, 4>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    case 1: return launch_block_t<NQ, 8, 2>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    case 2: return launch_block_t<NQ, 16, 1>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    default: return launch_block_t<NQ, W, C>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+  }
+}
+
 int launch_solve_block(const void* K16, int ld16, float expo, uint32_t vr_cap,
                        const SourceSel& s, const Targets& t, const SolveCtl& ctl,
-                       const float* u0, int64_t ldu, double* out, cudaStream_t st) {
+                       const float* u0, int64_t ldu, double* out, cudaStream_t st,
+                       int shape) {
   if (t.N <= 0) return 0;
   if (expo == 0.f || ld16 != block_panel_width(vr_cap)) return -1;
   switch (ld16 / 128) {
-    case 1: return launch_block_t<1, WMD_BLK_W1, WMD_BLK_C1>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
-    case 2: return launch_block_t<2, WMD_BLK_W2, WMD_BLK_C2>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
-    case 3: return launch_block_t<3, WMD_BLK_W3, WMD_BLK_C3>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
-    case 4: return launch_block_t<4, WMD_BLK_W4, WMD_BLK_C4>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    case 1: return launch_nq_default<1, WMD_BLK_W1, WMD_BLK_C1>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st, shape);
+    case 2: return launch_nq_default<2, WMD_BLK_W2, WMD_BLK_C2>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st, shape);
+    case 3: return launch_nq_default<3, WMD_BLK_W3, WMD_BLK_C3>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st, shape);
+    case 4: return launch_nq_default<4, WMD_BLK_W4, WMD_BLK_C4>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st, shape);
     default: return -1;
   }
 }

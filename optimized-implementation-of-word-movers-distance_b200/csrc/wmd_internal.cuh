@@ -187,9 +187,14 @@ int launch_solve(const float* K, const float* KM, int ld, float expo,
 int block_panel_width(uint32_t vr_cap);
 int launch_panel_to_bf16(const float* K, int ld, void* K16, int ld16, uint64_t V,
                          const uint32_t* vr, int num_sms, cudaStream_t st);
+// shape: index of a launch shape (0 .. block_shape_count()-1) or -1 for the
+// build-time default of the panel width.
 int launch_solve_block(const void* K16, int ld16, float expo, uint32_t vr_cap,
                        const SourceSel& s, const Targets& t, const SolveCtl& ctl,
-                       const float* u0, int64_t ldu, double* out, cudaStream_t st);
+                       const float* u0, int64_t ldu, double* out, cudaStream_t st,
+                       int shape = -1);
+int block_shape_count();
+const char* block_shape_name(int shape);
 
 // Learned warm start (warmstart.cu: training, ws_infer.cu: inference).
 // Parameter vector layout (FP32), for embedding width d:

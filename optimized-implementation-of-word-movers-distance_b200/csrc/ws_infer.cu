@@ -80,7 +80,8 @@ struct Params {
 };
 
 __host__ __device__ inline size_t smem_bytes() {
-  return 1024 + (size_t)kTileA + kW2 + (size_t)(3 * H + 2 * H) * 4 + 2 * BM * 4 + 64;
+  return 1024 + (size_t)kTileA + kW2 + (size_t)(3 * H + 2 * H) * 4 + 2 * BM * 4 +
+         2 * BM * 3 * 4 + 64;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) ws_init_kernel(const Params p,
@@ -94,7 +95,8 @@ __global__ void __launch_bounds__(kThreads, 1) ws_init_kernel(const Params p,
   float* sb2 = sWs + 3 * H;
   float* sw3 = sb2 + H;
   float* red = sw3 + H;                             // [2][BM]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(red + 2 * BM);
+  float* sst = red + 2 * BM;                        // [2][BM][3] M statistics
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sst + 2 * BM * 3);
   uint64_t* full = bars;      // producers -> MMA: A tile written
   uint64_t* done = bars + 1;  // MMA -> producers: accumulator ready, A free
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
@@ -163,24 +165,43 @@ __global__ void __launch_bounds__(kThreads, 1) ws_init_kernel(const Params p,
       const bool ok = pr < total;
       const int64_t j = ok ? pr / p.vr : 0;
       const int i = ok ? (int)(pr % p.vr) : 0;
-      // M statistics over the document's words.
-      float mn = 0.f, mean = 0.f, mx = 0.f;
+      // M statistics over the document's words: the two threads of a row
+      // (one per column half) take alternate words, four independent loads
+      // in flight each, and combine through shared memory.
+      int n = 0;
+      float lo = INFINITY, hi = -INFINITY, sm = 0.f;
       if (ok) {
         const int64_t b = p.col_ptr[j];
-        const int n = (int)(p.col_ptr[j + 1] - b);
-        float lo = INFINITY, hi = -INFINITY, sm = 0.f;
-        for (int k = 0; k < n; ++k) {
-          const float kv = p.K[(size_t)p.ent[b + k].x * p.ld + i];
+        n = (int)(p.col_ptr[j + 1] - b);
+        auto acc = [&](float kv) {
           const float Mv = fmaxf(__logf(fmaxf(kv, 1e-38f)) / p.expo, 0.f);
           lo = fminf(lo, Mv);
           hi = fmaxf(hi, Mv);
           sm += Mv;
+        };
+        int k = half;
+        for (; k + 6 < n; k += 8) {
+          const uint32_t w0 = p.ent[b + k].x, w1 = p.ent[b + k + 2].x;
+          const uint32_t w2 = p.ent[b + k + 4].x, w3 = p.ent[b + k + 6].x;
+          const float k0 = p.K[(size_t)w0 * p.ld + i], k1 = p.K[(size_t)w1 * p.ld + i];
+          const float k2 = p.K[(size_t)w2 * p.ld + i], k3 = p.K[(size_t)w3 * p.ld + i];
+          acc(k0);
+          acc(k1);
+          acc(k2);
+          acc(k3);
         }
-        if (n > 0) {
-          mn = lo;
-          mx = hi;
-          mean = sm / (float)n;
-        }
+        for (; k < n; k += 2) acc(p.K[(size_t)p.ent[b + k].x * p.ld + i]);
+      }
+      sst[(half * BM + row) * 3 + 0] = lo;
+      sst[(half * BM + row) * 3 + 1] = hi;
+      sst[(half * BM + row) * 3 + 2] = sm;
+      asm volatile("bar.sync 1, 256;" ::: "memory");
+      float mn = 0.f, mean = 0.f, mx = 0.f;
+      if (n > 0) {
+        const int o = ((half ^ 1) * BM + row) * 3;
+        mn = fminf(lo, sst[o]);
+        mx = fmaxf(hi, sst[o + 1]);
+        mean = (sm + sst[o + 2]) / (float)n;
       }
       // z1 -> GELU -> BF16 A tile (this thread: row `row`, columns c0..c0+127).
       const float* Ar = p.Asrc + (size_t)i * H;

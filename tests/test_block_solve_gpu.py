@@ -77,3 +77,28 @@ def test_block_solve_convergence_stopping(wmd, synth, oracle_mod):
     assert done.mean() > 0.9
     _check(out[0][done], conv[done], 2e-4)
     eng.close()
+
+
+def test_autotuned_launch_shape(wmd, synth, oracle_mod):
+    """The autotuner times every launch shape on the real panel and keeps the
+    fastest; any shape gives the same result within FP32 reordering, and the
+    chosen one is reproducible."""
+    p = synth.case(4000, 300, 400, 300, 8, 256, 40, 23)
+    ref = oracle_mod.sinkhorn(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                              p.row_inds, p.vals, p.lam, p.max_iter)
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.set_solve_precision("bf16")
+    eng.set_autotune(False)
+    a = eng.query(p.r, p.lam, p.max_iter)
+    assert eng.autotune_choices() == {}
+    eng.set_autotune(True)
+    b = eng.query(p.r, p.lam, p.max_iter)
+    ch = eng.autotune_choices()
+    assert list(ch) == [(384, False)] and "warps" in ch[(384, False)]
+    c = eng.query(p.r, p.lam, p.max_iter)
+    np.testing.assert_array_equal(b, c)
+    _check(b, ref)
+    assert rel_err(a, b).max() <= 1e-5
+    eng.close()
