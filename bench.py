@@ -509,6 +509,12 @@ def ours(a, rank, world, local):
         "stage_ms": {"select": sel_ms, "cdist": cd_ms, "solve": sv_ms},
         "bytes_model": "per iteration nnz*8 + nnz*v_r*4 + 2*N*v_r*4, final "
                        "nnz*8 + 2*nnz*v_r*4 + 8*N; cdist V*d*4 + 2*v_r*V*4",
+        "note": ("the solve's bytes model counts K-row gathers that the kernel "
+                 "serves from L2 and on-chip storage (the panel is L2-resident, "
+                 "a document's rows are reused across all passes), so frac > 1 "
+                 "is expected; DRAM traffic per launch is `traffic` (ncu), and "
+                 "the binding limit is FP32 issue/latency: fp32_frac")
+                if dominant == "solve_kernel" else None,
     }
 
     # e2e through the drop-in C ABI with pinned host buffers.
@@ -541,6 +547,7 @@ def ours(a, rank, world, local):
         dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
         dist.all_reduce(res_tot, op=dist.ReduceOp.MAX)
     e2e_value = p.N * world * a.e2e_steps / float(e2e_tot.item())
+    e2e_pcie_gbs = h2d * a.e2e_steps / float(e2e_tot.item()) / 1e9
     res_value = p.N * world * a.e2e_steps / float(res_tot.item())
     e2e_err = float(np.max(np.abs(res[:sub] - ref) / np.abs(ref)))
 
@@ -576,6 +583,7 @@ def ours(a, rank, world, local):
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "wmd_sinkhorn_fused_csc (drop-in, host buffers)",
+                    "h2d_gbs": e2e_pcie_gbs,
                     "resident_corpus_value": res_value,
                     "resident_corpus_h2d_bytes_per_step": p.V * 8,
                     "max_rel_err_vs_oracle": e2e_err},
