@@ -215,7 +215,10 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
         x[t] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       int k = r0;
-      // Four rows per step: two independent reduction chains in flight.
+      // Four rows per step: two independent reduction chains in flight
+      // (measured faster than converting each row to FP32 once and reusing
+      // it: the reductions' latency, not the instruction count, bounds a
+      // pass).
       for (; k + 2 < r1; k += 4) {
         uint2 qa[NQ], qb[NQ], qc[NQ], qd[NQ];
         float ca, cb, cc, cd;
