@@ -311,14 +311,19 @@ def extras(a, wmd, p, dev):
     eng.set_cdist_mode("fp32")
     eng.set_tolerance(1e-4)
     fn = lambda: eng.query_device(r_dev.data_ptr(), W["v_r"], p.lam, 5000, o.data_ptr())
-    dt = timed(eng, fn, 20)
-    it = eng.last_iterations()
-    ec = _rel(o[:sub].cpu().numpy(), conv)
-    out["single_source_converged"] = {
-        "tol_marginal_residual": 1e-4, "pairs_per_s": p.N / dt,
-        "iters_mean": float(it.mean()), "iters_max": int(it.max()),
-        "rel_err_vs_converged_fp64_max": float(ec.max()),
-        "oracle_iters_to_1e-9_mean": float(conv_it.mean())}
+    conv_out = {"tol_marginal_residual": 1e-4,
+                "oracle_iters_to_1e-9_mean": float(conv_it.mean())}
+    for omega in (1.0, 1.5):
+        eng.set_relaxation(omega)
+        dt = timed(eng, fn, 20)
+        it = eng.last_iterations()
+        ec = _rel(o[:sub].cpu().numpy(), conv)
+        conv_out[f"omega={omega}"] = {
+            "pairs_per_s": p.N / dt, "iters_mean": float(it.mean()),
+            "iters_max": int(it.max()),
+            "rel_err_vs_converged_fp64_max": float(ec.max())}
+    eng.set_relaxation(1.0)
+    out["single_source_converged"] = conv_out
     eng.close()
 
     # 3. batched queries: sources of the 512-source set (v_r ~ U[4,512])
@@ -361,6 +366,14 @@ def extras(a, wmd, p, dev):
     conv_b = {"sources": len(held), "tol_marginal_residual": 1e-4,
               "cold": {"pairs_per_s": len(held) * N / tc,
                        "iters_mean": float(itc.mean())}}
+    eng.set_relaxation(1.8)
+    t0 = time.perf_counter()
+    relx, itr = eng.query_batch(held, p.lam, 5000, want_iters=True)
+    tr = time.perf_counter() - t0
+    conv_b["cold_omega=1.8"] = {"pairs_per_s": len(held) * N / tr,
+                                "iters_mean": float(itr.mean()),
+                                "max_rel_diff_vs_cold": float(np.nanmax(_rel(relx, cold)))}
+    eng.set_relaxation(1.0)
     if not a.no_warm_start:
         train = [synth.source_doc(V, int(v), seed=1000 + q, cdf=cdf)
                  for q, v in enumerate(rng.integers(4, 513, a.ws_train_sources))]
@@ -377,6 +390,13 @@ def extras(a, wmd, p, dev):
         t0 = time.perf_counter()
         warm, itw = eng.query_batch(held, p.lam, 5000, want_iters=True)
         tw = time.perf_counter() - t0
+        eng.set_relaxation(1.8)
+        t0 = time.perf_counter()
+        wr, itwr = eng.query_batch(held, p.lam, 5000, want_iters=True)
+        twr = time.perf_counter() - t0
+        eng.set_relaxation(1.0)
+        conv_b["warm_omega=1.8"] = {"pairs_per_s": len(held) * N / twr,
+                                    "iters_mean": float(itwr.mean())}
         conv_b["warm"] = {"pairs_per_s": len(held) * N / tw,
                           "iters_mean": float(itw.mean()),
                           "max_rel_diff_vs_cold": float(np.nanmax(_rel(warm, cold))),

@@ -161,6 +161,13 @@ wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec);
  * beyond; -2 = not tuned yet, -1 = build-time default); the name of a shape
  * comes from wmd_block_shape_name. */
 wmd_status wmd_set_autotune(wmd_handle* h, int enable);
+
+/* Over-relaxed update u <- u^(1-omega) * u_hat^omega, 0 < omega < 2
+ * (default 1: the reference's iteration exactly).  Same fixed point; with
+ * per-document stopping (wmd_set_tolerance) 1 < omega < 2 reaches the
+ * tolerance in fewer updates on slowly converging documents (overrelaxed
+ * Sinkhorn-Knopp, Thibault et al. 2017).  No reference counterpart. */
+wmd_status wmd_set_relaxation(wmd_handle* h, double omega);
 wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes);
 const char* wmd_block_shape_name(int shape);
 

@@ -278,6 +278,10 @@ class Engine:
     def set_cdist_mode(self, mode: str):
         check(lib().wmd_set_cdist_mode(self._h, CDIST_MODES[mode]))
 
+    def set_relaxation(self, omega: float = 1.0):
+        """Over-relaxed u update (1 = the reference's iteration)."""
+        check(lib().wmd_set_relaxation(self._h, float(omega)))
+
     def set_autotune(self, enable: bool = True):
         check(lib().wmd_set_autotune(self._h, int(bool(enable))))
 

@@ -70,6 +70,7 @@ _SIGS = [
     ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_solve_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_set_relaxation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     ("wmd_autotune_choices", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("wmd_block_shape_name", ctypes.c_char_p, [ctypes.c_int]),
     ("wmd_ws_param_count", ctypes.c_uint64, [ctypes.c_uint64]),

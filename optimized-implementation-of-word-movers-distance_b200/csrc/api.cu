@@ -91,12 +91,13 @@ struct QueryKey {
   bool timing = false;
   uint64_t epoch = 0;
   float tol = 0.f;
+  float omega = 1.f;
   int prec = -1;
   const void* bufs[16] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
-          epoch == o.epoch && tol == o.tol && prec == o.prec))
+          epoch == o.epoch && tol == o.tol && omega == o.omega && prec == o.prec))
       return false;
     for (int i = 0; i < 16; ++i)
       if (bufs[i] != o.bufs[i]) return false;
@@ -152,6 +153,7 @@ struct wmd_handle {
   int64_t ws_rows = 0;
   std::vector<uint32_t> doc_len;  // host copy of the target lengths
   float tol = 0.f;  // per-document convergence tolerance (0: fixed count)
+  float omega = 1.f;  // over-relaxation of the u update (1: reference)
   unsigned* err_host = nullptr;      // pinned
   uint32_t* chunks_host = nullptr;   // pinned, grown with V
   size_t chunks_host_cap = 0;
@@ -508,6 +510,7 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->iters.as<int>();
+    ctl.omega = h->omega;
     if (ws) {
       n += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
                           h->ws_params.as<float>(), sel.S, sel.rinv, (int)cap,
@@ -550,6 +553,7 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.timing = h->timing;
   key.epoch = h->graph_epoch;
   key.tol = h->tol;
+  key.omega = h->omega;
   key.prec = (int)h->prec + (ws ? 2 : 0);
   {
     const DevBuf* used[16] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
@@ -799,6 +803,7 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->b_iters.as<int>() + s * N;
+    ctl.omega = h->omega;
     if (ws && vr > 0) {
       launches += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
                                  h->ws_params.as<float>(), sel.S, sel.rinv, (int)vr,
@@ -1018,6 +1023,14 @@ wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
   if (mode != WMD_CDIST_FP32 && mode != WMD_CDIST_BF16 && mode != WMD_CDIST_FP16)
     return fail(WMD_ERR_INVALID_ARG, "unknown cdist mode");
   h->mode = mode;
+  return WMD_OK;
+}
+
+wmd_status wmd_set_relaxation(wmd_handle* h, double omega) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (!(omega > 0.0 && omega < 2.0))
+    return fail(WMD_ERR_INVALID_ARG, "relaxation must be in (0, 2)");
+  h->omega = (float)omega;
   return WMD_OK;
 }
 

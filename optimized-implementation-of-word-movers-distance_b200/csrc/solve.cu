@@ -118,7 +118,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              const uint2* __restrict__ ent,
              const int32_t* __restrict__ order, int64_t N, int max_iter,
              float tol, int* __restrict__ iters_out, int srounds,
-             const float* __restrict__ u0, int64_t ldu,
+             const float* __restrict__ u0, int64_t ldu, float omega,
              double* __restrict__ out) {
   using Sh = SolveShape<LPW>;
   constexpr int WPS = Sh::WPS;
@@ -366,8 +366,9 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
 #pragma unroll
       for (int qq = 0; qq < LPW; ++qq) {
         const bool ok = (dmask >> qq) & 1u;
-        if (want_res && ok) res += fabsf(ubuf[32 * qq + lane] * tot[qq] - rw[qq]);
-        unew[qq] = ok ? __frcp_rn(rv[qq] * tot[qq]) : 0.f;
+        const float uo = ubuf[32 * qq + lane];
+        if (want_res && ok) res += fabsf(uo * tot[qq] - rw[qq]);
+        unew[qq] = ok ? relaxed_update(uo, __frcp_rn(rv[qq] * tot[qq]), omega) : 0.f;
       }
       if (want_res) {
 #pragma unroll
@@ -510,7 +511,7 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   if (grid < 1) grid = 1;
   solve_kernel<LPW, FROM_KM><<<(unsigned)grid, kWarps * 32, smem, st>>>(
       K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
-      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, out);
+      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, out);
   return 1;
 }
 

@@ -97,7 +97,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                    const int32_t* __restrict__ order, int64_t N, int max_iter,
                    float tol, int* __restrict__ iters_out,
                    const float* __restrict__ u0, int64_t ldu, int max_rows,
-                   double* __restrict__ out) {
+                   float omega, double* __restrict__ out) {
   using Sh = BlockShape<NQ, kBW>;
   constexpr int kBT = kBW * 32;
   constexpr int RL = Sh::RL;
@@ -259,8 +259,9 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
 #pragma unroll
           for (int w = 0; w < kBW; ++w) tot += xbuf[w * RL + D];
           if (D < vr) {
-            res += fabsf(src[D] * tot - rw[i]);
-            dst[D] = __frcp_rn(rv[i] * tot);
+            const float uo = src[D];
+            res += fabsf(uo * tot - rw[i]);
+            dst[D] = relaxed_update(uo, __frcp_rn(rv[i] * tot), omega);
           } else {
             dst[D] = 0.f;
           }
@@ -413,7 +414,7 @@ static int launch_block_t(const void* K16, int ld16, float expo,
   if (grid < 1) grid = 1;
   solve_block_kernel<NQ, kBW, kCPS><<<(unsigned)grid, kBW * 32, Sh::bytes(rows), st>>>(
       static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr,
-      t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows, out);
+      t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows, ctl.omega, out);
   return 1;
 }
 

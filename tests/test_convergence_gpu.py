@@ -38,3 +38,31 @@ def test_converged_solve_matches_fp64_oracle(wmd, synth, oracle_mod, tol):
                                 p.row_inds, p.vals, p.lam, 15)
     assert rel_err(fixed, ref15).max() <= 1e-5
     eng.close()
+
+
+@pytest.mark.parametrize("vr,prec", [(32, "fp32"), (200, "bf16")])
+def test_over_relaxation_same_fixed_point_fewer_updates(wmd, synth, oracle_mod, vr, prec):
+    """omega > 1 stops (residual <= 1e-5) within 1e-4 of the converged FP64
+    oracle like omega = 1, in fewer updates on average."""
+    p = synth.case(4000, 300, 300, vr, 8, 200, 60, 500 + vr)
+    conv = oracle_mod.sinkhorn_converged(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                                         p.row_inds, p.vals, p.lam, tol=1e-10,
+                                         max_iter_cap=50000)[0]
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.set_solve_precision(prec)
+    eng.set_tolerance(1e-5)
+    its = {}
+    for omega in (1.0, 1.6):
+        eng.set_relaxation(omega)
+        got = eng.query(p.r, p.lam, 5000)
+        it = eng.last_iterations()
+        done = it < 5000
+        assert done.mean() > 0.95
+        assert rel_err(got[done], conv[done]).max() <= 1e-4
+        its[omega] = it.mean()
+    assert its[1.6] < its[1.0], its
+    with pytest.raises(wmd.WMDError):
+        eng.set_relaxation(2.0)
+    eng.close()
