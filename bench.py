@@ -358,21 +358,30 @@ def extras(a, wmd, p, dev):
     rng = np.random.default_rng(11)
     held = [synth.source_doc(V, int(v), seed=5000 + q, cdf=cdf)
             for q, v in enumerate(rng.integers(4, 513, 16))]
-    eng.set_solve_precision("bf16")
     eng.set_tolerance(1e-4)
+    # the plain FP32 GPU path at the same criterion (the comparison point)
+    eng.set_solve_precision("fp32")
+    t0 = time.perf_counter()
+    plain, itp = eng.query_batch(held, p.lam, 5000, want_iters=True)
+    tp = time.perf_counter() - t0
+    eng.set_solve_precision("bf16")
     t0 = time.perf_counter()
     cold, itc = eng.query_batch(held, p.lam, 5000, want_iters=True)
     tc = time.perf_counter() - t0
     conv_b = {"sources": len(held), "tol_marginal_residual": 1e-4,
+              "plain_fp32": {"pairs_per_s": len(held) * N / tp,
+                             "iters_mean": float(itp.mean())},
               "cold": {"pairs_per_s": len(held) * N / tc,
-                       "iters_mean": float(itc.mean())}}
+                       "iters_mean": float(itc.mean()),
+                       "max_rel_diff_vs_plain_fp32": float(np.nanmax(_rel(cold, plain)))}}
     eng.set_relaxation(1.8)
     t0 = time.perf_counter()
     relx, itr = eng.query_batch(held, p.lam, 5000, want_iters=True)
     tr = time.perf_counter() - t0
     conv_b["cold_omega=1.8"] = {"pairs_per_s": len(held) * N / tr,
                                 "iters_mean": float(itr.mean()),
-                                "max_rel_diff_vs_cold": float(np.nanmax(_rel(relx, cold)))}
+                                "max_rel_diff_vs_plain_fp32": float(np.nanmax(_rel(relx, plain))),
+                                "speedup_vs_plain_fp32": tp / tr}
     eng.set_relaxation(1.0)
     if not a.no_warm_start:
         train = [synth.source_doc(V, int(v), seed=1000 + q, cdf=cdf)
@@ -396,7 +405,8 @@ def extras(a, wmd, p, dev):
         twr = time.perf_counter() - t0
         eng.set_relaxation(1.0)
         conv_b["warm_omega=1.8"] = {"pairs_per_s": len(held) * N / twr,
-                                    "iters_mean": float(itwr.mean())}
+                                    "iters_mean": float(itwr.mean()),
+                                    "speedup_vs_plain_fp32": tp / twr}
         conv_b["warm"] = {"pairs_per_s": len(held) * N / tw,
                           "iters_mean": float(itw.mean()),
                           "max_rel_diff_vs_cold": float(np.nanmax(_rel(warm, cold))),
