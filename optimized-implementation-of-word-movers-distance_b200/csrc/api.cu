@@ -202,6 +202,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
     return fail(WMD_ERR_INVALID_ARG, "set_embeddings: bad argument");
   if (V > 0xFFFFFFFFull)
     return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^32 words");
+  if (d > 65536) return fail(WMD_ERR_UNSUPPORTED, "embedding width above 65536");
   wmd_status s = bind(h);
   if (s) return s;
   const size_t n = (size_t)V * d;
