@@ -225,25 +225,19 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     running += ktot;
     __syncthreads();
   }
-  // Gather the selected rows of E32: all threads of the block over the
-  // (row, column) elements, so that a chunk holding most of a Zipf source's
-  // words (the frequent, low ids) copies them with every load in flight.
-  // (32-bit index math: running <= 1024 rows of d < 2^22 columns.)
-  const unsigned du = (unsigned)d;
-  const unsigned nel = running * du;
-  for (unsigned e = threadIdx.x; e < nel; e += kSelectThreads) {
-    const unsigned s = e / du, k = e - s * du;
+  // Gather the selected rows of E32 (one warp per selected word).
+  for (unsigned s = warp; s < running; s += kSelectThreads / 32) {
     const uint32_t pos = list_pos[s];
-    if (pos < cap) S[(uint64_t)pos * d + k] = E32[(uint64_t)list_id[s] * d + k];
-  }
-  for (unsigned s = threadIdx.x; s < running; s += kSelectThreads)
-    if (list_pos[s] < cap) nS[list_pos[s]] = nE[list_id[s]];
-  if (S16) {  // 16-bit copy for the tensor-core cost panel
-    const unsigned dpu = (unsigned)dp, n16 = running * dpu;
-    for (unsigned e = threadIdx.x; e < n16; e += kSelectThreads) {
-      const unsigned s = e / dpu, k = e - s * dpu;
-      const uint32_t pos = list_pos[s];
-      if (pos < cap) S16[(uint64_t)pos * dp + k] = E16[(uint64_t)list_id[s] * dp + k];
+    if (pos >= cap) continue;
+    const uint64_t id = list_id[s];
+    const float* src = E32 + id * d;
+    float* dst = S + (uint64_t)pos * d;
+    for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
+    if (lane == 0) nS[pos] = nE[id];
+    if (S16) {  // 16-bit copy for the tensor-core cost panel
+      const unsigned short* s16 = E16 + id * (uint64_t)dp;
+      unsigned short* d16 = S16 + (uint64_t)pos * dp;
+      for (int k = lane; k < dp; k += 32) d16[k] = s16[k];
     }
   }
 }
