@@ -170,6 +170,10 @@ wmd_status wmd_set_autotune(wmd_handle* h, int enable);
 wmd_status wmd_set_relaxation(wmd_handle* h, double omega);
 wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes);
 const char* wmd_block_shape_name(int shape);
+/* Pin the block solve to one shape (0..5; 3-5 = the tensor-core form with
+ * 1, 2 or 4 CTAs per SM, whose longest documents run on the CUDA cores),
+ * -1 = the build-time default, -2 = back to the autotuner. */
+wmd_status wmd_set_block_shape(wmd_handle* h, int shape);
 
 /* One source document as a dense host histogram r[V] (the reference's form,
  * zeros skipped as sinkhorn_wmd_fused.cpp:45-63 does).  wmd_out: host, N. */

@@ -285,6 +285,12 @@ class Engine:
     def set_autotune(self, enable: bool = True):
         check(lib().wmd_set_autotune(self._h, int(bool(enable))))
 
+    def set_block_shape(self, shape: int):
+        """Pin the block solve's shape (0-2 CUDA-core launch shapes, 3-5 the
+        tensor-core form at 1, 2, 4 CTAs per SM, -1 build-time default,
+        -2 autotune)."""
+        check(lib().wmd_set_block_shape(self._h, int(shape)))
+
     def autotune_choices(self) -> dict:
         """{(panel width, beyond 64 MiB): chosen block-solve launch shape}."""
         a = (ctypes.c_int * 8)()

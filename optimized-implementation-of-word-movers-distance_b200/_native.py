@@ -73,6 +73,7 @@ _SIGS = [
     ("wmd_set_relaxation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     ("wmd_autotune_choices", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("wmd_block_shape_name", ctypes.c_char_p, [ctypes.c_int]),
+    ("wmd_set_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_ws_param_count", ctypes.c_uint64, [ctypes.c_uint64]),
     ("wmd_ws_init_params", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, c_f32p]),
     ("wmd_ws_build_training_set", ctypes.c_int,

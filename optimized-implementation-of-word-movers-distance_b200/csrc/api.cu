@@ -120,7 +120,11 @@ struct wmd_handle {
   // Launch-shape autotuner of the block solve: per (panel width, panel
   // beyond L2) the fastest shape measured on this handle's data.
   bool autotune = true;
+  int forced_shape = -2;  // wmd_set_block_shape (-2: none)
   int blk_shape[8] = {-2, -2, -2, -2, -2, -2, -2, -2};  // -2: not tuned yet
+  // Documents longer than the tensor-core solve's capacity, per panel width
+  // (-1: not counted yet for this target set).
+  int64_t tc_long[4][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
   // embeddings
   DevBuf E32, nE, E64_stage, E16;
   uint64_t V = 0, d = 0;
@@ -306,6 +310,8 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   h->have_T = true;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
+  for (auto& row : h->tc_long)
+    for (int64_t& x : row) x = -1;
   h->doc_len.resize(N);
   for (uint64_t j = 0; j < N; ++j) h->doc_len[j] = (uint32_t)(c->col_ptr[j + 1] - c->col_ptr[j]);
   h->graph_epoch++;
@@ -347,6 +353,31 @@ wmd_status csr_to_csc_host(const wmd_csr_double_t* a, std::vector<uint64_t>& cp,
   return WMD_OK;
 }
 
+// Documents of the target set longer than the tensor-core solve holds (they
+// come first in the length order).
+int64_t tc_long_count(wmd_handle* h, int ld16, int shape) {
+  const int w = (ld16 / 128 - 1) & 3, k = shape - 3;
+  if (h->tc_long[w][k] >= 0) return h->tc_long[w][k];
+  const uint32_t cap = (uint32_t)tc_solve_capacity(ld16, 1 << k);
+  int64_t c = 0;
+  for (uint32_t l : h->doc_len) c += l > cap ? 1 : 0;
+  h->tc_long[w][k] = c;
+  return c;
+}
+
+// The block solve in launch shape `shape` (3-5: tensor cores with 1, 2 or 4
+// CTAs per SM for the documents that fit, the build-time CUDA-core shape
+// for the longer ones).
+int launch_block_shape(wmd_handle* h, const void* K16, int ld16, float expo,
+                       uint32_t vr, const SourceSel& sel, const Targets& t,
+                       const SolveCtl& ctl, const float* u0, int64_t ldu,
+                       double* out, int shape) {
+  if (shape >= 3 && shape <= 5)
+    return launch_solve_tc(K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, h->stream,
+                           1 << (shape - 3), tc_long_count(h, ld16, shape));
+  return launch_solve_block(K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, h->stream, shape);
+}
+
 // Launch shape of the block solve for this panel: cached per (width, panel
 // beyond L2); when not yet known and the call may synchronise, every
 // candidate shape is timed on the real panel and target set (4 updates, CUDA
@@ -355,6 +386,7 @@ wmd_status csr_to_csc_host(const wmd_csr_double_t* a, std::vector<uint64_t>& cp,
 int block_shape_for(wmd_handle* h, const void* K16, int ld16, float expo,
                     uint32_t vr, const SourceSel& sel, const Targets& t,
                     const SolveCtl& ctl, double* out, bool can_sync) {
+  if (h->forced_shape != -2) return h->forced_shape;
   const int key = ((ld16 / 128 - 1) & 3) * 2 + ((size_t)h->V * ld16 * 2 > (64u << 20) ? 1 : 0);
   if (h->blk_shape[key] != -2) return h->blk_shape[key];
   if (!h->autotune || !can_sync) return -1;
@@ -371,10 +403,10 @@ int block_shape_for(wmd_handle* h, const void* K16, int ld16, float expo,
   float best = 1e30f;
   int bi = -1;
   for (int sh = 0; sh < block_shape_count(); ++sh) {
-    if (launch_solve_block(K16, ld16, expo, vr, sel, t, c2, nullptr, 0, out, h->stream, sh) < 0)
+    if (launch_block_shape(h, K16, ld16, expo, vr, sel, t, c2, nullptr, 0, out, sh) < 0)
       continue;  // shape unavailable (shared-memory budget)
     cudaEventRecord(a, h->stream);
-    launch_solve_block(K16, ld16, expo, vr, sel, t, c2, nullptr, 0, out, h->stream, sh);
+    launch_block_shape(h, K16, ld16, expo, vr, sel, t, c2, nullptr, 0, out, sh);
     cudaEventRecord(b, h->stream);
     float ms = 0.f;
     if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess &&
@@ -527,8 +559,8 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
                                 h->sms, h->stream);
       const int shape = block_shape_for(h, h->K16.p, ld16, expo, cap, sel, t, ctl,
                                         out_dev, !capturing);
-      const int ls = launch_solve_block(h->K16.p, ld16, expo, cap, sel, t, ctl,
-                                        ctl.u0, ctl.ldu, out_dev, h->stream, shape);
+      const int ls = launch_block_shape(h, h->K16.p, ld16, expo, cap, sel, t, ctl,
+                                        ctl.u0, ctl.ldu, out_dev, shape);
       if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "block solve unavailable");
       n += ls;
     } else {
@@ -821,8 +853,8 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                                        sel.vr, h->sms, h->stream);
       const int shape = block_shape_for(h, h->K16.p, ld16, expo, vr, sel, t, ctl,
                                         h->b_out.as<double>() + s * N, true);
-      ls = launch_solve_block(h->K16.p, ld16, expo, vr, sel, t, ctl, ctl.u0, ctl.ldu,
-                              h->b_out.as<double>() + s * N, h->stream, shape);
+      ls = launch_block_shape(h, h->K16.p, ld16, expo, vr, sel, t, ctl, ctl.u0, ctl.ldu,
+                              h->b_out.as<double>() + s * N, shape);
     } else {
       ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
                         h->b_out.as<double>() + s * N, h->stream);
@@ -1039,6 +1071,15 @@ wmd_status wmd_set_autotune(wmd_handle* h, int enable) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
   h->autotune = enable != 0;
   for (int& x : h->blk_shape) x = -2;
+  h->graph_epoch++;
+  return WMD_OK;
+}
+
+wmd_status wmd_set_block_shape(wmd_handle* h, int shape) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (shape < -2 || shape >= block_shape_count())
+    return fail(WMD_ERR_INVALID_ARG, "unknown block-solve shape");
+  h->forced_shape = shape;
   h->graph_epoch++;
   return WMD_OK;
 }
@@ -1700,6 +1741,8 @@ wmd_status wmd_set_targets_edges(wmd_handle* h, const uint64_t* words,
   h->have_T = true;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
+  for (auto& row : h->tc_long)
+    for (int64_t& x : row) x = -1;
   h->doc_len.resize(N);
   for (uint64_t j = 0; j < N; ++j) h->doc_len[j] = (uint32_t)(cp[j + 1] - cp[j]);
   h->graph_epoch++;

@@ -420,11 +420,16 @@ static int launch_block_t(const void* K16, int ld16, float expo,
 
 // Launch shapes the autotuner chooses from (warps per CTA, CTAs per SM).
 // shape < 0 selects the build-time table above.
-int block_shape_count() { return 3; }
+// Indices 3-5 are the tensor-core form (solve_tc.cu) with 1, 2 or 4 CTAs
+// per SM, launched by the caller.
+int block_shape_count() { return 6; }
 const char* block_shape_name(int shape) {
   static const char* names[] = {"4 warps x 4 CTAs/SM", "8 warps x 2 CTAs/SM",
-                                "16 warps x 1 CTA/SM"};
-  return shape >= 0 && shape < 3 ? names[shape] : "build-time table";
+                                "16 warps x 1 CTA/SM",
+                                "tensor cores, 1 CTA/SM (longest documents on CUDA cores)",
+                                "tensor cores, 2 CTAs/SM (longest documents on CUDA cores)",
+                                "tensor cores, 4 CTAs/SM (longest documents on CUDA cores)"};
+  return shape >= 0 && shape < 6 ? names[shape] : "build-time table";
 }
 
 template <int NQ, int W, int C>

@@ -207,6 +207,15 @@ int launch_solve_block(const void* K16, int ld16, float expo, uint32_t vr_cap,
                        int shape = -1);
 int block_shape_count();
 const char* block_shape_name(int shape);
+// Tensor-core form of the block solve (solve_tc.cu): documents up to
+// tc_solve_capacity(ld16) rows on the tensor cores; order[0 .. n_long), the
+// longer ones, on the CUDA-core block kernel.
+// cps: CTAs sharing an SM (the row capacity shrinks with it).
+int tc_solve_capacity(int ld16, int cps);
+int launch_solve_tc(const void* K16, int ld16, float expo, uint32_t vr_cap,
+                    const SourceSel& s, const Targets& t, const SolveCtl& ctl,
+                    const float* u0, int64_t ldu, double* out, cudaStream_t st,
+                    int cps, int64_t n_long);
 
 // Learned warm start (warmstart.cu: training, ws_infer.cu: inference).
 // Parameter vector layout (FP32), for embedding width d:

@@ -102,3 +102,40 @@ def test_autotuned_launch_shape(wmd, synth, oracle_mod):
     _check(b, ref)
     assert rel_err(a, b).max() <= 1e-5
     eng.close()
+
+
+@pytest.mark.parametrize("vr", [65, 200, 300, 512])
+def test_tensor_core_block_solve(wmd, synth, oracle_mod, vr):
+    """The tensor-core form (mma.sync BF16 with the three-way split of u and
+    v) against the FP64 oracle and the CUDA-core form on the same BF16 panel:
+    documents up to 256 words, so at the widest panel the longest ones run on
+    the CUDA cores; also the converged mode with a warm start absent."""
+    p = synth.case(4000, 300, 300, vr, 8, 256, 40, 700 + vr, empty_every=41)
+    ref = oracle_mod.sinkhorn(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                              p.row_inds, p.vals, p.lam, p.max_iter)
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.set_solve_precision("bf16")
+    eng.set_block_shape(0)
+    simt = eng.query(p.r, p.lam, p.max_iter)
+    for shape in (3, 4, 5):  # 1, 2, 4 CTAs per SM (different length splits)
+        eng.set_block_shape(shape)
+        tc = eng.query(p.r, p.lam, p.max_iter)
+        _check(tc, ref)
+        np.testing.assert_array_equal(tc, eng.query(p.r, p.lam, p.max_iter))
+        assert rel_err(tc, simt).max() <= 2e-5
+    eng.set_tolerance(1e-5)
+    eng.set_block_shape(4)
+    a = eng.query(p.r, p.lam, 3000)
+    ita = eng.last_iterations()
+    eng.set_block_shape(0)
+    b = eng.query(p.r, p.lam, 3000)
+    itb = eng.last_iterations()
+    # Slowly converging documents cross the tolerance a few updates apart
+    # (the residual falls slowly there); the results agree to the
+    # tolerance's scale.
+    assert np.mean(np.abs(ita - itb) <= 2 + 0.02 * itb) > 0.95
+    done = (ita < 3000) & (itb < 3000)
+    assert rel_err(a[done], b[done]).max() <= 1e-4
+    eng.close()
