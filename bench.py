@@ -267,6 +267,19 @@ def _rel(a, b):
     return e
 
 
+def _one_per_width(rs):
+    """One source of each BF16 panel width class (v_r rounded up to 128), so
+    that a warm-up call leaves the one-time launch-shape tuning of every class
+    out of the timed call."""
+    seen, out = set(), []
+    for r in rs:
+        w = (np.count_nonzero(r) + 127) // 128
+        if w not in seen:
+            seen.add(w)
+            out.append(r)
+    return out
+
+
 def extras(a, wmd, p, dev):
     import torch
     import oracle
@@ -344,7 +357,7 @@ def extras(a, wmd, p, dev):
                "nnz": int(cpb[-1])}
     for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
         eng.set_solve_precision(prec)
-        eng.query_batch(rs[:2], p.lam, 15)
+        eng.query_batch(_one_per_width(rs), p.lam, 15)
         t0 = time.perf_counter()
         res = eng.query_batch(rs, p.lam, 15)
         dt = time.perf_counter() - t0
@@ -446,7 +459,7 @@ def large_vocab(wmd, dev):
     for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
         eng.set_solve_precision(prec)
         eng.set_timing(True)
-        eng.query_batch(rs[:1], 10.0, 15)
+        eng.query_batch(_one_per_width(rs), 10.0, 15)
         t0 = time.perf_counter()
         out = eng.query_batch(rs, 10.0, 15)
         dt = time.perf_counter() - t0
