@@ -96,7 +96,8 @@ def test_autotuned_launch_shape(wmd, synth, oracle_mod):
     eng.set_autotune(True)
     b = eng.query(p.r, p.lam, p.max_iter)
     ch = eng.autotune_choices()
-    assert list(ch) == [(384, False)] and "warps" in ch[(384, False)]
+    names = {wmd.lib().wmd_block_shape_name(i).decode() for i in range(6)}
+    assert list(ch) == [(384, False)] and ch[(384, False)] in names
     c = eng.query(p.r, p.lam, p.max_iter)
     np.testing.assert_array_equal(b, c)
     _check(b, ref)
