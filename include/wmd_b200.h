@@ -123,7 +123,13 @@ typedef struct wmd_handle wmd_handle;
 typedef enum wmd_cdist_mode {
   WMD_CDIST_FP32 = 0, /* FP32 CUDA-core GEMM form, near pairs recomputed */
   WMD_CDIST_BF16 = 1, /* tcgen05 tensor cores, BF16 operands, FP32 accum */
-  WMD_CDIST_FP16 = 2  /* tcgen05 tensor cores, FP16 operands, FP32 accum */
+  WMD_CDIST_FP16 = 2, /* tcgen05 tensor cores, FP16 operands, FP32 accum */
+  /* tcgen05 tensor cores on the FP32 embeddings: each operand split into a
+   * TF32 high part and its FP32 remainder, three products (hi*hi + hi*lo +
+   * lo*hi) accumulated in FP32: FP32-accurate, near pairs recomputed as in
+   * WMD_CDIST_FP32.  Widths d that are not a multiple of 4 (or too wide for
+   * the tile) use the FP32 CUDA-core panel instead. */
+  WMD_CDIST_TF32X3 = 3
 } wmd_cdist_mode;
 
 wmd_status wmd_create(wmd_handle** out, int device);

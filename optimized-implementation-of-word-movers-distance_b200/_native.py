@@ -23,7 +23,7 @@ STATUS = {
     6: "WMD_ERR_UNSUPPORTED",
 }
 
-CDIST_MODES = {"fp32": 0, "bf16": 1, "fp16": 2}
+CDIST_MODES = {"fp32": 0, "bf16": 1, "fp16": 2, "tf32x3": 3}
 
 
 class WMDError(RuntimeError):

@@ -472,8 +472,10 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   t.nnz = (int64_t)h->nnz;
   if (cap > 1024)
     return fail(WMD_ERR_UNSUPPORTED, "more than 1024 non-zero source words");
-  const bool tcm = h->mode != WMD_CDIST_FP32;
+  const bool tcm = h->mode == WMD_CDIST_BF16 || h->mode == WMD_CDIST_FP16;
   const bool bf16 = h->mode == WMD_CDIST_BF16;
+  // Split-TF32 form; widths it cannot tile use the FP32 CUDA-core panel.
+  const bool x3 = h->mode == WMD_CDIST_TF32X3 && tc_tile_n_x3(cap, d) != 0;
   const int dp = tc_padded_width(d);
   int launches = 0;
   if (tcm) {
@@ -524,8 +526,9 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
                        tcm ? h->E16.p : nullptr, tcm ? h->sel_S16.p : nullptr, dp);
     CK(record(1, capturing));
     CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
-    if (tcm) {
-      const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16,
+    if (tcm || x3) {
+      const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
+                                     h->E16.p, h->sel_S16.p,
                                      h->E32.as<float>(), h->nE.as<float>(), V, d,
                                      sel, expo, h->K.as<float>(), KMp, ld, near,
                                      h->err_dev.as<unsigned>(), h->sms, h->stream);
@@ -736,8 +739,9 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
       rinv[e] = (float)(1.0 / src_w[e]);
     }
   }
-  const bool tcm = h->mode != WMD_CDIST_FP32;
+  const bool tcm = h->mode == WMD_CDIST_BF16 || h->mode == WMD_CDIST_FP16;
   const bool bf16 = h->mode == WMD_CDIST_BF16;
+  const bool x3 = h->mode == WMD_CDIST_TF32X3 && tc_tile_n_x3(vr_max, d) != 0;
   const int dp = tc_padded_width(d);
   if (tcm && tc_tile_n(vr_max, d) == 0)
     return fail(WMD_ERR_UNSUPPORTED, "embedding width too large for the tensor-core panel");
@@ -816,8 +820,9 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                                       tcm ? h->E16.p : nullptr,
                                       tcm ? h->sel_S16.p : nullptr, dp, h->stream);
     CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
-    if (tcm) {
-      const int lc = launch_cdist_tc(h->E16.p, h->sel_S16.p, bf16, h->E32.as<float>(),
+    if (tcm || x3) {
+      const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
+                                     h->E16.p, h->sel_S16.p, h->E32.as<float>(),
                                      h->nE.as<float>(), V, d, sel, expo,
                                      h->K.as<float>(), KMp, ld, near,
                                      h->err_dev.as<unsigned>(), h->sms, h->stream);
@@ -1053,7 +1058,8 @@ wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* a) {
 
 wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
-  if (mode != WMD_CDIST_FP32 && mode != WMD_CDIST_BF16 && mode != WMD_CDIST_FP16)
+  if (mode != WMD_CDIST_FP32 && mode != WMD_CDIST_BF16 && mode != WMD_CDIST_FP16 &&
+      mode != WMD_CDIST_TF32X3)
     return fail(WMD_ERR_INVALID_ARG, "unknown cdist mode");
   h->mode = mode;
   return WMD_OK;

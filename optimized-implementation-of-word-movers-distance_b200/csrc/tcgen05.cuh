@@ -11,6 +11,7 @@ namespace wmd {
 namespace tc {
 
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound per wait
+constexpr uint32_t kSuspendNs = 100000;  // try_wait suspend hint (upper bound)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -35,7 +36,10 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
                : "memory");
 }
 // Waits for the phase of parity `par` to complete.  Bounded: returns false
-// (and flags the error word) after kWaitNs of wall-clock time.
+// (and flags the error word) after kWaitNs of wall-clock time.  Each try_wait
+// carries a suspend-time hint, so a waiting thread sleeps in hardware until
+// the phase completes instead of spinning on issue slots that the MMA-issuing
+// and converting warps of the same SM sub-partition need.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par,
                                           unsigned* err) {
   const uint32_t a = smem_u32(bar);
@@ -44,10 +48,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par,
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(done)
-        : "r"(a), "r"(par)
+        : "r"(a), "r"(par), "r"(kSuspendNs)
         : "memory");
     if (done) return true;
     if ((i & 63) == 0) {
@@ -79,8 +83,8 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   d |= (uint64_t)2u << 61;               // SWIZZLE_128B
   return d;
 }
-// Instruction descriptor of kind::f16: FP32 accumulate, A/B K-major,
-// fmt 0 = FP16, 1 = BF16 (both operands), M x N tile.
+// Instruction descriptor of kind::f16 / kind::tf32: FP32 accumulate, A/B
+// K-major, fmt 0 = FP16, 1 = BF16, 2 = TF32 (both operands), M x N tile.
 __host__ __device__ constexpr uint32_t make_idesc(int fmt, int M, int N) {
   return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) |
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
@@ -91,6 +95,15 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b,
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+          d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b,
+                                         uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
           d_tmem),
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }

@@ -139,14 +139,18 @@ int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
                       const SourceSel& s, float expo, float* K, float* KM,
                       int ld, const NearList& near, cudaStream_t st);
 
-// Tensor-core cost panel (cdist_tc.cu).  E16/S16 rows are dp = d rounded up
-// to 8 16-bit elements.  Returns launches, or -1 if unsupported (tensor maps
-// or shared-memory budget).
+// Tensor-core cost panel (cdist_tc.cu).  Forms: 16-bit operands (E16/S16
+// rows are dp = d rounded up to 8 elements), or the FP32-accurate split-TF32
+// form that reads E32/S directly (E16/S16 unused; needs d % 4 == 0).
+// Returns launches, or -1 if unsupported (tensor maps or shared-memory
+// budget).
+enum TcForm { TC_FP16 = 0, TC_BF16 = 1, TC_TF32X3 = 2 };
 int tc_padded_width(uint64_t d);
 int tc_tile_n(uint32_t cap, uint64_t d);
+int tc_tile_n_x3(uint32_t cap, uint64_t d);  // 0 = form unsupported
 int launch_to16(const float* E32, uint64_t rows, uint64_t d, void* E16,
                 bool bf16, cudaStream_t st);
-int launch_cdist_tc(const void* E16, const void* S16, bool bf16,
+int launch_cdist_tc(int form, const void* E16, const void* S16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
                     const NearList& near, unsigned* err, int num_sms,

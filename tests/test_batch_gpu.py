@@ -20,7 +20,7 @@ def problem(synth):
     return vecs, cp, ri, vv, rs
 
 
-@pytest.mark.parametrize("mode", ["fp32", "fp16"])
+@pytest.mark.parametrize("mode", ["fp32", "fp16", "tf32x3"])
 def test_batch_equals_single_queries(wmd, oracle_mod, problem, mode):
     vecs, cp, ri, vv, rs = problem
     eng = wmd.Engine()
@@ -33,7 +33,7 @@ def test_batch_equals_single_queries(wmd, oracle_mod, problem, mode):
     for k, r in enumerate(rs):
         single = eng.query(r, 10.0, 15)
         np.testing.assert_array_equal(out[k], single)
-        if mode == "fp32":
+        if mode in ("fp32", "tf32x3"):
             ref = oracle_mod.sinkhorn(r, vecs.astype(np.float64), cp, ri, vv, 10.0, 15)
             np.testing.assert_array_equal(np.isnan(out[k]), np.isnan(ref))
             assert rel_err(out[k], ref).max() <= 1e-5
