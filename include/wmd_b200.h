@@ -110,6 +110,15 @@ wmd_status wmd_sinkhorn_nonfused_csc(const double* r, const double* vecs,
                                      uint64_t word2vec_word_embedding_size,
                                      const wmd_csc_double_t* c_csc);
 
+/* Host -> device bytes moved by the calling thread's last successful drop-in
+ * call above (target matrix, r, embedding rows).  When `vecs` lies in one
+ * pinned, device-mapped host allocation (cudaHostAlloc / cudaMallocHost /
+ * cudaHostRegister), the GPU reads only the rows of the words that occur in
+ * the target matrix or in r, directly from host memory; otherwise the whole
+ * V x d matrix is copied.  Results are the same either way.  No reference
+ * counterpart (a measurement aid). */
+uint64_t wmd_dropin_h2d_bytes(void);
+
 /* ---------------------------------------------------------------------------
  * Handle API: embeddings and target set stay resident on the GPU across
  * queries (the serving form of the same solve).  No reference counterpart:

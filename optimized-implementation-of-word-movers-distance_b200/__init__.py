@@ -72,6 +72,13 @@ def sinkhorn_wmd_csc(r, vecs, col_ptr, row_inds, vals, lamda, max_iter,
     return out
 
 
+def dropin_h2d_bytes() -> int:
+    """Host -> device bytes of this thread's last drop-in call: with the
+    embeddings in pinned host memory only the rows of words that occur in the
+    targets or the source cross the bus (``wmd_dropin_h2d_bytes``)."""
+    return int(lib().wmd_dropin_h2d_bytes())
+
+
 def _csr_call(fn, r, vecs, lamda, max_iter, row_ptr, col_inds, vals, num_docs):
     r, vecs = _f64(r), _f64(vecs)
     row_ptr, col_inds, vals = _u64(row_ptr), _u64(col_inds), _f64(vals)

@@ -133,6 +133,7 @@ _SIGS = [
     ("wmd_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("wmd_last_error", ctypes.c_char_p, []),
     ("wmd_abi_version", ctypes.c_int, []),
+    ("wmd_dropin_h2d_bytes", ctypes.c_uint64, []),
 ]
 
 _lib = None

@@ -12,6 +12,8 @@
 #include <random>
 #include <vector>
 
+#include <cuda.h>
+
 #include "wmd_b200.h"
 #include "wmd_internal.cuh"
 
@@ -127,6 +129,8 @@ struct wmd_handle {
   int64_t tc_long[4][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
   // embeddings
   DevBuf E32, nE, E64_stage, E16;
+  DevBuf need, need_count;  // needed-rows upload of the drop-in calls
+  uint64_t dropin_h2d = 0;  // bytes the last drop-in call moved host -> device
   uint64_t V = 0, d = 0;
   bool have_E = false;
   int e16_fmt = -1;  // format E16 holds (1 bf16, 2 fp16), -1 = stale
@@ -523,9 +527,9 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     CK(record(0, capturing));
     n += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d, sel,
                        h->err_dev.as<unsigned>(), h->stream,
-                       tcm ? h->E16.p : nullptr, tcm ? h->sel_S16.p : nullptr, dp);
+                       tcm ? h->E16.p : nullptr, tcm ? h->sel_S16.p : nullptr, dp,
+                       near.count);  // the selection also zeroes the near-pair count
     CK(record(1, capturing));
-    CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
     if (tcm || x3) {
       const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
                                      h->E16.p, h->sel_S16.p,
@@ -643,7 +647,7 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
 // Query from a dense HOST histogram: copy, count the non-zeros on the GPU,
 // size the panels for exactly that many source words, solve, copy back.
 wmd_status query_host(wmd_handle* h, const double* r, float expo, int max_iter,
-                      double* wmd_out) {
+                      double* wmd_out, bool r_on_device = false) {
   if (!h->have_E || !h->have_T)
     return fail(WMD_ERR_INVALID_ARG, "embeddings and targets must be set first");
   if (h->tV != h->V)
@@ -663,8 +667,9 @@ wmd_status query_host(wmd_handle* h, const double* r, float expo, int max_iter,
   }
   wmd_status s = clear_err(h);
   if (s) return s;
-  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice,
-                     h->stream));
+  if (!r_on_device)
+    CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream));
   // Count pass alone first: v_r sizes every later buffer.
   uint32_t* counts = h->sel_chunks.as<uint32_t>();
   const int lc = launch_select_count(h->r_dev.as<double>(), V, counts,
@@ -878,6 +883,81 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   return finish(h);
 }
 
+// Device view of [p, p + bytes) when the whole range lies in one pinned,
+// device-mapped host allocation (the runtime reports host memory and the
+// driver's allocation range covers the span); null otherwise.
+typedef CUresult (*PtrAttrFn)(void*, CUpointer_attribute, CUdeviceptr);
+PtrAttrFn ptr_attr_fn() {
+  static PtrAttrFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PtrAttrFn>(p);
+  }
+  return fn;
+}
+
+const void* mapped_host_range(const void* p, size_t bytes) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  PtrAttrFn f = ptr_attr_fn();
+  if (!f) return nullptr;
+  const CUdeviceptr dp = (CUdeviceptr)(uintptr_t)a.devicePointer;
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  if (f(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, dp) != CUDA_SUCCESS ||
+      f(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, dp) != CUDA_SUCCESS)
+    return nullptr;
+  if (dp < start || dp - start > size || bytes > size - (size_t)(dp - start))
+    return nullptr;
+  return a.devicePointer;
+}
+
+// Drop-in embeddings from device-mapped host memory: only the rows of the
+// words the query can touch (the targets already set, the source words of r)
+// cross the bus.  Leaves r uploaded in r_dev.  The handle's E then holds
+// zeros for every other word, so it is only valid for this target set and
+// this r — which is how the drop-in calls use their private handle.
+wmd_status set_embeddings_needed(wmd_handle* h, const double* vecs_mapped,
+                                 const double* r, uint64_t V, uint64_t d) {
+  if (V > 0xFFFFFFFFull)
+    return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^32 words");
+  if (d > 65536) return fail(WMD_ERR_UNSUPPORTED, "embedding width above 65536");
+  if (!h->have_T || h->tV != V)
+    return fail(WMD_ERR_INVALID_ARG, "targets must be set first");
+  const size_t n = (size_t)V * d;
+  CK(h->E32.ensure(n * sizeof(float)));
+  CK(h->nE.ensure((size_t)V * sizeof(float)));
+  CK(h->need.ensure((size_t)V));
+  CK(h->need_count.ensure(2 * sizeof(unsigned long long)));
+  CK(h->r_dev.ensure(V * sizeof(double)));
+  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice,
+                     h->stream));
+  int launches = launch_gather_needed_f64(
+      vecs_mapped, V, d, h->ent.as<uint2>(), h->nnz, h->r_dev.as<double>(),
+      h->need.as<unsigned char>(), h->E32.as<float>(), h->nE.as<float>(),
+      h->need_count.as<unsigned long long>(), h->stream);
+  CK(cudaGetLastError());
+  h->V = V;
+  h->d = d;
+  h->have_E = true;
+  h->e16_fmt = -1;
+  h->ws_docs_ready = false;
+  for (int& x : h->blk_shape) x = -2;
+  h->graph_epoch++;
+  h->last_launches = launches;
+  return WMD_OK;
+}
+
 // Per-host-thread default handle for the drop-in calls.
 struct TlHandle {
   wmd_handle* h = nullptr;
@@ -915,15 +995,38 @@ wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
   wmd_handle* h = nullptr;
   wmd_status s = default_handle(&h);
   if (s) return s;
-  s = set_embeddings(h, vecs, V, d, 0, true);
-  if (s) return s;
-  const int le = h->last_launches;
-  s = set_targets_csc(h, c);
-  if (s) return s;
-  const int lt = h->last_launches;
-  s = query_host(h, r, expo, max_iter, WMD);
+  const uint64_t csc_bytes = (N + 1) * 8 + c->nnz * 16 + N * 4;  // + order
+  const void* vmap = mapped_host_range(vecs, (size_t)V * d * sizeof(double));
+  int le = 0, lt = 0;
+  if (vmap) {
+    // Pinned, device-mapped embeddings: targets first, then only the rows
+    // they (and the source) need are read over the bus.
+    s = set_targets_csc(h, c);
+    if (s) return s;
+    lt = h->last_launches;
+    s = set_embeddings_needed(h, static_cast<const double*>(vmap), r, V, d);
+    if (s) return s;
+    le = h->last_launches;
+  } else {
+    s = set_embeddings(h, vecs, V, d, 0, true);
+    if (s) return s;
+    le = h->last_launches;
+    s = set_targets_csc(h, c);
+    if (s) return s;
+    lt = h->last_launches;
+  }
+  s = query_host(h, r, expo, max_iter, WMD, vmap != nullptr);
   if (s) return s;
   h->last_launches += le + lt;
+  uint64_t rows = V;
+  if (vmap) {
+    unsigned long long cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, h->need_count.p, sizeof(cnt), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    rows = cnt;
+  }
+  h->dropin_h2d = csc_bytes + V * 8 + rows * d * 8;
   return WMD_OK;
 }
 
@@ -1240,6 +1343,8 @@ wmd_status wmd_sinkhorn_nonfused(const double* r, const double* vecs,
   return dropin_csr(r, vecs, WMD, (float)(-lamda), max_iter, data_vocab_size,
                     num_docs, word2vec_word_embedding_size, c_csr);
 }
+
+uint64_t wmd_dropin_h2d_bytes(void) { return tl_handle.h ? tl_handle.h->dropin_h2d : 0; }
 
 wmd_status wmd_sinkhorn_fused_csc(const double* r, const double* vecs,
                                   double* WMD, double lamda, int max_iter,

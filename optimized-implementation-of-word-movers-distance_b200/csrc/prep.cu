@@ -66,6 +66,82 @@ int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
 }
 
 // ---------------------------------------------------------------------------
+// Needed rows only (drop-in calls whose FP64 embeddings sit in pinned,
+// device-mapped host memory): flag the words a query can touch — every target
+// word and every source word (r != 0) — then read exactly those rows over the
+// bus, convert them to FP32 with their norms, and zero the rest (a zero row
+// is finite and never near any source row, so the cost panel's unused rows
+// stay harmless; the solve never gathers them).
+// ---------------------------------------------------------------------------
+__global__ void mark_needed_kernel(const uint2* __restrict__ ent, uint64_t nnz,
+                                   const double* __restrict__ r, uint64_t V,
+                                   unsigned char* __restrict__ need) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nnz) need[ent[i].x] = 1;  // ids were range-checked when packed
+  if (i < V && r[i] != 0.0) need[i] = 1;
+}
+
+__global__ void gather_convert_f64_kernel(const double* __restrict__ src, uint64_t V,
+                                          uint64_t d,
+                                          const unsigned char* __restrict__ need,
+                                          float* __restrict__ E32,
+                                          float* __restrict__ nE,
+                                          unsigned long long* __restrict__ nrows) {
+  const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= V) return;
+  float* o = E32 + row * d;
+  if (!need[row]) {
+    for (uint64_t k = lane; k < d; k += 32) o[k] = 0.f;
+    if (lane == 0) nE[row] = 0.f;
+    return;
+  }
+  if (lane == 0) atomicAdd(nrows, 1ull);  // rows read over the bus
+  const double* s = src + row * d;
+  double acc = 0.0;
+  if (d <= 512) {
+    // All of a lane's loads before any use: one bus round trip per row.
+    double v[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t k = (uint64_t)lane + 32u * t;
+      v[t] = k < d ? s[k] : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t k = (uint64_t)lane + 32u * t;
+      const float f = (float)v[t];
+      if (k < d) o[k] = f;
+      acc += (double)f * (double)f;
+    }
+  } else {
+    for (uint64_t k = lane; k < d; k += 32) {
+      const float f = (float)s[k];
+      o[k] = f;
+      acc += (double)f * (double)f;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) nE[row] = (float)acc;
+}
+
+int launch_gather_needed_f64(const double* src_mapped, uint64_t V, uint64_t d,
+                             const uint2* ent, uint64_t nnz, const double* r_dev,
+                             unsigned char* need, float* E32, float* nE,
+                             unsigned long long* nrows, cudaStream_t st) {
+  const int threads = 256;
+  cudaMemsetAsync(need, 0, V, st);
+  cudaMemsetAsync(nrows, 0, sizeof(unsigned long long), st);
+  const uint64_t n = nnz > V ? nnz : V;
+  mark_needed_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(
+      ent, nnz, r_dev, V, need);
+  gather_convert_f64_kernel<<<(unsigned)((V * 32 + threads - 1) / threads), threads, 0,
+                              st>>>(src_mapped, V, d, need, E32, nE, nrows);
+  return 2;
+}
+
+// ---------------------------------------------------------------------------
 // Targets: validate a CSC triple and pack it for the solver.  The checks are
 // those of the reference driver's MTX reader (sinkhorn_wmd_fused.cpp:474-478):
 // indices in range and values > 0; plus consistent column pointers.
@@ -142,11 +218,37 @@ __device__ __forceinline__ unsigned block_sum_u32(unsigned v, unsigned* red) {
   return t;
 }
 
+// Copy of one embedding row by a warp.  For d <= 512 every lane issues all
+// its loads before its stores (one memory round trip for the row instead of
+// one per 32 elements: the rows are cold in L2 when a query starts).
+__device__ __forceinline__ void copy_row(const float* __restrict__ src,
+                                         float* __restrict__ dst, uint64_t d,
+                                         int lane) {
+  if (d <= 512) {
+    float v[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t k = (uint64_t)lane + 32u * t;
+      v[t] = k < d ? __ldg(src + k) : 0.f;
+    }
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t k = (uint64_t)lane + 32u * t;
+      if (k < d) dst[k] = v[t];
+    }
+  } else {
+    for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
+  }
+}
+
 __global__ void __launch_bounds__(kSelectThreads)
 select_count_kernel(const double* __restrict__ r, uint64_t V,
                     uint32_t* __restrict__ chunk_counts,
-                    unsigned* __restrict__ err) {
+                    unsigned* __restrict__ err, unsigned* __restrict__ zero_word) {
   __shared__ unsigned red[33];
+  // A counter of a later kernel of the same query (the near-pair list), reset
+  // here instead of by a separate memset on the stream.
+  if (zero_word && blockIdx.x == 0 && threadIdx.x == 0) *zero_word = 0u;
   const uint64_t base = (uint64_t)blockIdx.x * kSelectChunk;
   unsigned cnt = 0;
   bool neg = false;
@@ -180,6 +282,14 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
   __shared__ uint32_t list_pos[kSelectChunk];
   __shared__ uint32_t list_id[kSelectChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * kSelectChunk;
+  // This chunk's weights first: their loads overlap the offset computation.
+  double rv[kSelectPerThread];
+#pragma unroll
+  for (int k = 0; k < kSelectPerThread; ++k) {
+    const uint64_t i = base + (uint64_t)k * kSelectThreads + threadIdx.x;
+    rv[k] = i < V ? r[i] : 0.0;
+  }
 
   // Offset of this chunk = selected count of all chunks before it.
   unsigned before = 0, all = 0;
@@ -195,12 +305,11 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     if (total > cap) atomicOr(err, ERR_VR_CAP);
   }
 
-  const uint64_t base = (uint64_t)blockIdx.x * kSelectChunk;
   unsigned running = 0;
+#pragma unroll
   for (int k = 0; k < kSelectPerThread; ++k) {
     const uint64_t i = base + (uint64_t)k * kSelectThreads + threadIdx.x;
-    double v = 0.0;
-    if (i < V) v = r[i];
+    const double v = rv[k];
     const bool sel = (i < V) && (v != 0.0);
     const unsigned bal = __ballot_sync(0xffffffffu, sel);
     if (lane == 0) warp_off[warp] = __popc(bal);
@@ -232,7 +341,7 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     const uint64_t id = list_id[s];
     const float* src = E32 + id * d;
     float* dst = S + (uint64_t)pos * d;
-    for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
+    copy_row(src, dst, d, lane);
     if (lane == 0) nS[pos] = nE[id];
     if (S16) {  // 16-bit copy for the tensor-core cost panel
       const unsigned short* s16 = E16 + id * (uint64_t)dp;
@@ -245,16 +354,17 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
 int launch_select_count(const double* r, uint64_t V, uint32_t* chunk_counts,
                         unsigned* err, cudaStream_t st) {
   select_count_kernel<<<select_num_chunks(V), kSelectThreads, 0, st>>>(
-      r, V, chunk_counts, err);
+      r, V, chunk_counts, err, nullptr);
   return 1;
 }
 
 int launch_select(const double* r, uint64_t V, const float* E32,
                   const float* nE, uint64_t d, const SourceSel& s,
                   unsigned* err, cudaStream_t st, const void* E16, void* S16,
-                  int dp) {
+                  int dp, unsigned* zero_word) {
   const int nchunks = select_num_chunks(V);
-  select_count_kernel<<<nchunks, kSelectThreads, 0, st>>>(r, V, s.chunk_counts, err);
+  select_count_kernel<<<nchunks, kSelectThreads, 0, st>>>(r, V, s.chunk_counts, err,
+                                                          zero_word);
   select_write_kernel<<<nchunks, kSelectThreads, 0, st>>>(
       r, V, E32, nE, d, nchunks, s.chunk_counts, s.cap, s.ids, s.rinv, s.S,
       s.nS, s.vr, err, static_cast<const unsigned short*>(E16),
@@ -281,7 +391,7 @@ __global__ void gather_sources_kernel(const uint32_t* __restrict__ ids, int coun
   const uint64_t id = ids[w];
   const float* src = E32 + id * d;
   float* dst = S + (uint64_t)w * d;
-  for (uint64_t k = lane; k < d; k += 32) dst[k] = src[k];
+  copy_row(src, dst, d, lane);
   if (lane == 0) nS[w] = nE[id];
   if (S16) {
     const unsigned short* s16 = E16 + id * (uint64_t)dp;

@@ -104,6 +104,14 @@ int launch_embed_convert_f64(const double* src, uint64_t V, uint64_t d,
                              float* E32, float* nE, cudaStream_t st);
 int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
                        cudaStream_t st);
+// Rows of the words a query can touch (target words in `ent`, source words
+// r_dev != 0) read from device-mapped host memory and converted; all other
+// rows zeroed.  `need` is V bytes of scratch; *nrows receives the number of
+// rows read.
+int launch_gather_needed_f64(const double* src_mapped, uint64_t V, uint64_t d,
+                             const uint2* ent, uint64_t nnz, const double* r_dev,
+                             unsigned char* need, float* E32, float* nE,
+                             unsigned long long* nrows, cudaStream_t st);
 
 // Targets: validated packing of a CSC triple into (col_ptr, ent).
 int launch_pack_targets(const uint64_t* col_ptr_in, const uint64_t* rows_in,
@@ -117,10 +125,12 @@ int launch_select_count(const double* r, uint64_t V, uint32_t* chunk_counts,
 
 // Source selection r != 0 (ascending id) + gather of the source rows (and,
 // when S16 is given, of their 16-bit copies [cap][dp] from E16 [V][dp]).
+// zero_word, when given, is set to 0 by the first kernel (the near-pair
+// counter of the cost panel that follows).
 int launch_select(const double* r, uint64_t V, const float* E32,
                   const float* nE, uint64_t d, const SourceSel& s,
                   unsigned* err, cudaStream_t st, const void* E16 = nullptr,
-                  void* S16 = nullptr, int dp = 0);
+                  void* S16 = nullptr, int dp = 0, unsigned* zero_word = nullptr);
 
 // Top-k nearest documents (topk.cu): stable ascending order of the FP64
 // scores, ties by index, NaN last.  1 <= k <= 1024.
