@@ -177,11 +177,19 @@ wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec);
  * comes from wmd_block_shape_name. */
 wmd_status wmd_set_autotune(wmd_handle* h, int enable);
 
-/* Over-relaxed update u <- u^(1-omega) * u_hat^omega, 0 < omega < 2
- * (default 1: the reference's iteration exactly).  Same fixed point; with
- * per-document stopping (wmd_set_tolerance) 1 < omega < 2 reaches the
- * tolerance in fewer updates on slowly converging documents (overrelaxed
- * Sinkhorn-Knopp, Thibault et al. 2017).  No reference counterpart. */
+/* Over-relaxed iteration, 0 < omega < 2 (default 1: the reference's
+ * iteration exactly): both half-steps are relaxed, v <- v^(1-omega) *
+ * v_hat^omega and u <- u^(1-omega) * u_hat^omega, each target word keeping
+ * its previous v.  Same fixed point; with per-document stopping
+ * (wmd_set_tolerance, whose residual then also counts the target-side
+ * marginal) 1 < omega < 2 reaches the tolerance in far fewer updates on
+ * slowly converging documents (overrelaxed Sinkhorn-Knopp: Thibault et al.
+ * 2017; Lehmann et al. 2021).  A per-document guard steps omega halfway back
+ * to 1 whenever the residual grows 100-fold over its best, and restarts the
+ * document unrelaxed from the cold start if it stops being finite.  Applies
+ * only with per-document stopping (tolerance > 0): a fixed update count runs
+ * the reference's iteration.  Ignored for lambda = 0.  No reference
+ * counterpart. */
 wmd_status wmd_set_relaxation(wmd_handle* h, double omega);
 wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes);
 const char* wmd_block_shape_name(int shape);

@@ -95,13 +95,13 @@ struct QueryKey {
   float tol = 0.f;
   float omega = 1.f;
   int prec = -1;
-  const void* bufs[16] = {};  // every device buffer the graph reads or writes
+  const void* bufs[17] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
           epoch == o.epoch && tol == o.tol && omega == o.omega && prec == o.prec))
       return false;
-    for (int i = 0; i < 16; ++i)
+    for (int i = 0; i < 17; ++i)
       if (bufs[i] != o.bufs[i]) return false;
     return true;
   }
@@ -142,6 +142,7 @@ struct wmd_handle {
   // per query
   DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_S16, sel_vr, sel_chunks,
       K, KM, K16, out_dev, err_dev, near_pairs, near_count, iters;
+  DevBuf vstate;  // each target word's previous v (over-relaxed solves)
   // batched queries
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
   // top-k
@@ -499,6 +500,8 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
   CK(h->near_count.ensure(sizeof(unsigned)));
   CK(h->iters.ensure((size_t)std::max<uint64_t>(h->N, 1) * sizeof(int)));
+  if (h->omega != 1.f)
+    CK(h->vstate.ensure((size_t)std::max<uint64_t>(h->nnz, 1) * sizeof(float)));
   NearList near;
   near.pairs = h->near_pairs.as<uint2>();
   near.count = h->near_count.as<unsigned>();
@@ -550,7 +553,8 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->iters.as<int>();
-    ctl.omega = h->omega;
+    ctl.omega = h->tol > 0.f ? h->omega : 1.f;  // relaxation needs stopping
+    ctl.vstate = ctl.omega != 1.f ? h->vstate.as<float>() : nullptr;
     if (ws) {
       n += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
                           h->ws_params.as<float>(), sel.S, sel.rinv, (int)cap,
@@ -596,11 +600,11 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.omega = h->omega;
   key.prec = (int)h->prec + (ws ? 2 : 0);
   {
-    const DevBuf* used[16] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+    const DevBuf* used[17] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
                               &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
                               &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16,
-                              &h->ws_Asrc, &h->ws_u0};
-    for (int i = 0; i < 16; ++i) key.bufs[i] = used[i]->p;
+                              &h->ws_Asrc, &h->ws_u0, &h->vstate};
+    for (int i = 0; i < 17; ++i) key.bufs[i] = used[i]->p;
   }
   if (!h->use_graphs) {
     int n = 0;
@@ -756,6 +760,8 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   CK(h->b_vr.ensure(S * sizeof(uint32_t)));
   CK(h->b_out.ensure(S * N * sizeof(double)));
   CK(h->b_iters.ensure(S * N * sizeof(int)));
+  if (h->omega != 1.f)
+    CK(h->vstate.ensure((size_t)std::max<uint64_t>(h->nnz, 1) * sizeof(float)));
   CK(h->sel_S.ensure((size_t)vr_max * d * sizeof(float)));
   CK(h->sel_nS.ensure((size_t)vr_max * sizeof(float)));
   CK(h->K.ensure((size_t)V * ld_max * sizeof(float)));
@@ -846,7 +852,8 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->b_iters.as<int>() + s * N;
-    ctl.omega = h->omega;
+    ctl.omega = h->tol > 0.f ? h->omega : 1.f;  // relaxation needs stopping
+    ctl.vstate = ctl.omega != 1.f ? h->vstate.as<float>() : nullptr;
     if (ws && vr > 0) {
       launches += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
                                  h->ws_params.as<float>(), sel.S, sel.rinv, (int)vr,

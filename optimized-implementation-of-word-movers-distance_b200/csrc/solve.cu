@@ -109,7 +109,7 @@ struct SolveShape {
   }
 };
 
-template <int LPW, bool FROM_KM>
+template <int LPW, bool FROM_KM, bool RLX>
 __global__ void __launch_bounds__(kWarps * 32, WMD_SOLVE_CTAS_PER_SM)
 solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              float expo, const uint32_t* __restrict__ vr_dev,
@@ -119,7 +119,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              const int32_t* __restrict__ order, int64_t N, int max_iter,
              float tol, int* __restrict__ iters_out, int srounds,
              const float* __restrict__ u0, int64_t ldu, float omega,
-             double* __restrict__ out) {
+             float* __restrict__ vstate, double* __restrict__ out) {
   using Sh = SolveShape<LPW>;
   constexpr int WPS = Sh::WPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -164,6 +164,9 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     n = (int)(col_ptr[j + 1] - b);
   }
   for (; idx < N; idx += total_warps) {
+    RelaxGuard rg;  // over-relaxation of this document (RLX instantiations)
+    rg.init(omega);
+    float resv = 0.f;  // this lane's c-side residual of the current pass
     const int64_t nidx = idx + total_warps;
     int64_t jn = 0;
     if (nidx < N) jn = order ? (int64_t)__ldg(&order[nidx]) : nidx;
@@ -270,6 +273,24 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     // v = c / s for a real word; exactly 0 for the padding words (c = 0 and
     // a zero row), which would otherwise give 0/0.
     auto weight = [](float c, float s) { return c != 0.f ? __fdividef(c, s) : 0.f; };
+    // v of word k in a pass; over-relaxed (RLX) against the word's previous v
+    // (vold, prefetched by vold_at with the word's row), which lane q = 0 of
+    // the word's group keeps in vstate and broadcasts.
+    auto vold_at = [&](int k) -> float {
+      if constexpr (RLX) return (q == 0 && k < n && !rg.vfirst) ? vstate[b + k] : 0.f;
+      else return 0.f;
+    };
+    auto vweight = [&](float c, float s, int k, float vold) -> float {
+      if constexpr (!RLX) {
+        return weight(c, s);
+      } else {
+        float v = 0.f;
+        if (q == 0 && k < n)
+          v = relaxed_v_pre(c, s, vold, vstate + b + k, rg.vfirst, rg.omega, resv);
+        if constexpr (LPW > 1) v = __shfl_sync(0xffffffffu, v, lane & ~(LPW - 1));
+        return v;
+      }
+    };
     // Sum the x slices of all word slots: lane writes its 32 values as row
     // `lane` of a 32x32 buffer (chunk-swizzled), then lane L sums column L for
     // each of its LPW dimension groups: tot[qq] is dimension 32*qq + L.
@@ -311,38 +332,48 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     };
     // One pass of v = c ./ (K^T u), x += K v over all rounds of the document.
     auto pass = [&](const float2 (&u2)[16], float2 (&x2)[16]) {
+      if constexpr (RLX) resv = 0.f;
 #pragma unroll
       for (int t = 0; t < 16; ++t) x2[t] = make_float2(0.f, 0.f);
       {
-        float sreg[RR];
+        float sreg[RR], oreg[RR];
+#pragma unroll
+        for (int t = 0; t < RR; ++t) oreg[t] = vold_at(t * WPS + g);
 #pragma unroll
         for (int t = 0; t < RR; ++t) sreg[t] = dot(reg[t], u2);
 #pragma unroll
-        for (int t = 0; t < RR; ++t) axpy(reg[t], weight(creg[t], sreg[t]), x2);
+        for (int t = 0; t < RR; ++t)
+          axpy(reg[t], vweight(creg[t], sreg[t], t * WPS + g, oreg[t]), x2);
       }
       constexpr int U = WMD_SOLVE_UNROLL;
       int t = 0;
       for (; t + U <= sr; t += U) {
         Row ra[U];
-        float ca[U], sa[U];
+        float ca[U], sa[U], oa[U];
 #pragma unroll
-        for (int i = 0; i < U; ++i) load_staged(t + i, ra[i], ca[i]);
+        for (int i = 0; i < U; ++i) {
+          load_staged(t + i, ra[i], ca[i]);
+          oa[i] = vold_at((rr + t + i) * WPS + g);
+        }
 #pragma unroll
         for (int i = 0; i < U; ++i) sa[i] = dot(ra[i], u2);
 #pragma unroll
-        for (int i = 0; i < U; ++i) axpy(ra[i], weight(ca[i], sa[i]), x2);
+        for (int i = 0; i < U; ++i)
+          axpy(ra[i], vweight(ca[i], sa[i], (rr + t + i) * WPS + g, oa[i]), x2);
       }
       for (; t < sr; ++t) {
         Row ra;
         float ca;
         load_staged(t, ra, ca);
-        axpy(ra, weight(ca, dot(ra, u2)), x2);
+        const float oa = vold_at((rr + t) * WPS + g);
+        axpy(ra, vweight(ca, dot(ra, u2), (rr + t) * WPS + g, oa), x2);
       }
       for (int l = 0; l < lr; ++l) {
         Row ra;
         float ca;
         load_global(K, (rr + sr + l) * WPS + g, ra, ca);
-        axpy(ra, weight(ca, dot(ra, u2)), x2);
+        const float oa = vold_at((rr + sr + l) * WPS + g);
+        axpy(ra, vweight(ca, dot(ra, u2), (rr + sr + l) * WPS + g, oa), x2);
       }
     };
 
@@ -363,12 +394,14 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       float tot[LPW];
       reduce_slots(x2, tot);
       float res = 0.f;
+      if constexpr (RLX) res = resv;
 #pragma unroll
       for (int qq = 0; qq < LPW; ++qq) {
         const bool ok = (dmask >> qq) & 1u;
         const float uo = ubuf[32 * qq + lane];
         if (want_res && ok) res += fabsf(uo * tot[qq] - rw[qq]);
-        unew[qq] = ok ? relaxed_update(uo, __frcp_rn(rv[qq] * tot[qq]), omega) : 0.f;
+        unew[qq] = ok ? relaxed_update(uo, __frcp_rn(rv[qq] * tot[qq]), RLX ? rg.omega : omega)
+                      : 0.f;
       }
       if (want_res) {
 #pragma unroll
@@ -396,12 +429,20 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       broadcast_u(uval, u2);
       res = use_warm ? rwm : rc;
       it = 1;
+      if constexpr (RLX) rg.vfirst = true;  // the stored v are the last candidate's
     }
     while (it < max_iter && !(it > 0 && tol > 0.f && res <= tol)) {
       float uval[LPW];
-      res = step(uval, tol > 0.f);
-      broadcast_u(uval, u2);
+      res = step(uval, tol > 0.f || RLX);
       ++it;
+      if constexpr (RLX) {
+        bool reset_u = false;
+        if (rg.step(res, it, &reset_u) && reset_u) {
+#pragma unroll
+          for (int qq = 0; qq < LPW; ++qq) uval[qq] = ((dmask >> qq) & 1u) ? (float)vr : 0.f;
+        }
+      }
+      broadcast_u(uval, u2);
     }
     if (iters_out && lane == 0) iters_out[j] = it;
 
@@ -476,7 +517,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   }
 }
 
-template <int LPW, bool FROM_KM>
+template <int LPW, bool FROM_KM, bool RLX>
 static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
                           const SourceSel& s, const Targets& t,
                           const SolveCtl& ctl, double* out, cudaStream_t st) {
@@ -495,7 +536,7 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
     const size_t per_round = (size_t)Sh::WPS * (Sh::RL * 4 + 4);
     int sr = per_warp > fixed ? (int)((per_warp - fixed) / per_round) : 0;
     while (sr > 0 && Sh::warp_bytes(sr) > per_warp) --sr;
-    cudaFuncSetAttribute(solve_kernel<LPW, FROM_KM>,
+    cudaFuncSetAttribute(solve_kernel<LPW, FROM_KM, RLX>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(kWarps * Sh::warp_bytes(sr)));
     int sms = 0;
@@ -509,22 +550,22 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   int64_t grid = (int64_t)sms_cache[dev] * kBlocksPerSm;
   if (grid > want) grid = want;
   if (grid < 1) grid = 1;
-  solve_kernel<LPW, FROM_KM><<<(unsigned)grid, kWarps * 32, smem, st>>>(
+  solve_kernel<LPW, FROM_KM, RLX><<<(unsigned)grid, kWarps * 32, smem, st>>>(
       K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
-      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, out);
+      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, ctl.vstate, out);
   return 1;
 }
 
-template <bool FROM_KM>
+template <bool FROM_KM, bool RLX>
 static int dispatch_solve(const float* K, const float* KM, int ld, float expo,
                           uint32_t vr_cap, const SourceSel& s, const Targets& t,
                           const SolveCtl& c, double* out, cudaStream_t st) {
-  if (vr_cap <= 32) return launch_solve_t<1, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
-  if (vr_cap <= 64) return launch_solve_t<2, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
-  if (vr_cap <= 128) return launch_solve_t<4, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
-  if (vr_cap <= 256) return launch_solve_t<8, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
-  if (vr_cap <= 512) return launch_solve_t<16, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
-  if (vr_cap <= 1024) return launch_solve_t<32, FROM_KM>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 32) return launch_solve_t<1, FROM_KM, RLX>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 64) return launch_solve_t<2, FROM_KM, RLX>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 128) return launch_solve_t<4, FROM_KM, RLX>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 256) return launch_solve_t<8, FROM_KM, RLX>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 512) return launch_solve_t<16, FROM_KM, RLX>(K, KM, ld, expo, s, t, c, out, st);
+  if (vr_cap <= 1024) return launch_solve_t<32, FROM_KM, RLX>(K, KM, ld, expo, s, t, c, out, st);
   return -1;
 }
 
@@ -532,9 +573,14 @@ int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
                  const SolveCtl& ctl, double* out, cudaStream_t st) {
   if (t.N <= 0) return 0;
+  // lambda = 0 (KM read from a panel: K = 1 everywhere) runs unrelaxed.
   if (KM)
-    return dispatch_solve<true>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
-  return dispatch_solve<false>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
+    return dispatch_solve<true, false>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
+  if (ctl.omega != 1.f) {
+    if (!ctl.vstate) return -1;
+    return dispatch_solve<false, true>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
+  }
+  return dispatch_solve<false, false>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);
 }
 
 }  // namespace wmd

@@ -87,7 +87,7 @@ struct BlockShape {
   }
 };
 
-template <int NQ, int kBW, int kCPS>
+template <int NQ, int kBW, int kCPS, bool RLX>
 __global__ void __launch_bounds__(kBW * 32, kCPS)
 solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                    const uint32_t* __restrict__ vr_dev,
@@ -97,7 +97,8 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                    const int32_t* __restrict__ order, int64_t N, int max_iter,
                    float tol, int* __restrict__ iters_out,
                    const float* __restrict__ u0, int64_t ldu, int max_rows,
-                   float omega, double* __restrict__ out) {
+                   float omega, float* __restrict__ vstate,
+                   double* __restrict__ out) {
   using Sh = BlockShape<NQ, kBW>;
   constexpr int kBT = kBW * 32;
   constexpr int RL = Sh::RL;
@@ -129,6 +130,12 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     const int n = (int)(col_ptr[j + 1] - b);
     const int ns = n < max_rows ? n : max_rows;  // rows staged in shared memory
     const bool warm = u0 != nullptr && max_iter > 0;
+    // Over-relaxation of both half-steps (vstate: each word's previous v),
+    // compiled only into the RLX instantiations.
+    constexpr bool relax = RLX;
+    RelaxGuard g;
+    g.init(omega);
+    float resv = 0.f;  // this thread's c-side residual of the current pass
 
     __syncthreads();  // the previous document is done with shared memory
     for (int k = tid; k < ns; k += kBT) sEnt[k] = __ldg(&ent[b + k]);
@@ -187,9 +194,24 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       return keep;
     };
     auto weight = [](float c, float s) { return c != 0.f ? __fdividef(c, s) : 0.f; };
-    // v of a row pair from its pair_sum: (v_a, v_b) in every lane.
-    auto pair_weights = [&](float s, float ca, float cb, float2& va, float2& vb) {
-      const float vm = weight(lo ? ca : cb, s);
+    // v of a row pair (rows ka, ka + 1) from its pair_sum: (v_a, v_b) in
+    // every lane.  Relaxed: lanes 0 and 16 own the rows' states (vold: the
+    // row's previous v, prefetched by vold_of).
+    auto vold_of = [&](int kr) -> float {
+      return (relax && !g.vfirst && (lane & 15) == 0 && kr < r1) ? vstate[b + kr] : 0.f;
+    };
+    auto pair_weights = [&](float s, float ca, float cb, int ka, float vold, float2& va,
+                            float2& vb) {
+      float vm;
+      if (relax) {
+        float v = 0.f;
+        if ((lane & 15) == 0)
+          v = relaxed_v_pre(lo ? ca : cb, s, vold, vstate + b + ka + (lo ? 0 : 1),
+                            g.vfirst, g.omega, resv);
+        vm = __shfl_sync(0xffffffffu, v, lane & 16);
+      } else {
+        vm = weight(lo ? ca : cb, s);
+      }
       const float vo = __shfl_xor_sync(0xffffffffu, vm, 16);
       va = make_float2(lo ? vm : vo, lo ? vm : vo);
       vb = make_float2(lo ? vo : vm, lo ? vo : vm);
@@ -209,6 +231,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     // Returns the marginal residual of `src` (CTA-uniform) when `want_res`.
     auto pass = [&](const float* src, float* dst, bool want_res) -> float {
       float4 u[NQ], x[NQ];
+      resv = 0.f;
 #pragma unroll
       for (int t = 0; t < NQ; ++t) {
         u[t] = reinterpret_cast<const float4*>(src)[lane + 32 * t];
@@ -226,11 +249,12 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
         load_row(k + 1, qb, cb);
         load_row(k + 2, qc, cc);
         load_row(k + 3, qd, cd);
+        const float o0 = vold_of(k + (lo ? 0 : 1)), o1 = vold_of(k + 2 + (lo ? 0 : 1));
         const float s0 = pair_sum(dot(qa, u), dot(qb, u));
         const float s1 = pair_sum(dot(qc, u), dot(qd, u));
         float2 va, vb, vc, vd;
-        pair_weights(s0, ca, cb, va, vb);
-        pair_weights(s1, cc, cd, vc, vd);
+        pair_weights(s0, ca, cb, k, o0, va, vb);
+        pair_weights(s1, cc, cd, k + 2, o1, vc, vd);
         axpy(qa, va, x);
         axpy(qb, vb, x);
         axpy(qc, vc, x);
@@ -241,8 +265,9 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
         float ca, cb;
         load_row(k, qa, ca);
         load_row(k + 1, qb, cb);
+        const float o0 = vold_of(k + (lo ? 0 : 1));
         float2 va, vb;
-        pair_weights(pair_sum(dot(qa, u), dot(qb, u)), ca, cb, va, vb);
+        pair_weights(pair_sum(dot(qa, u), dot(qb, u)), ca, cb, k, o0, va, vb);
         axpy(qa, va, x);
         axpy(qb, vb, x);
       }
@@ -250,7 +275,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       for (int t = 0; t < NQ; ++t)
         reinterpret_cast<float4*>(xbuf + warp * RL)[lane + 32 * t] = x[t];
       __syncthreads();
-      float res = 0.f;
+      float res = resv;
 #pragma unroll
       for (int i = 0; i < DPT; ++i) {
         const int D = tid + i * kBT;
@@ -261,7 +286,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
           if (D < vr) {
             const float uo = src[D];
             res += fabsf(uo * tot - rw[i]);
-            dst[D] = relaxed_update(uo, __frcp_rn(rv[i] * tot), omega);
+            dst[D] = relaxed_update(uo, __frcp_rn(rv[i] * tot), g.omega);
           } else {
             dst[D] = 0.f;
           }
@@ -284,7 +309,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     float* cur = ubufA;
     int it = 0;
     float res = 0.f;
-    const bool want_res = tol > 0.f;
+    const bool want_res = tol > 0.f || relax;
     if (warm) {
       const float rc = pass(ubufA, ubufA, true);
       const float rwm = pass(ubufB, ubufB, true);
@@ -294,10 +319,16 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       cur = use_warm ? ubufB : ubufA;
       res = use_warm ? rwm : rc;
       it = 1;
+      g.vfirst = true;  // the stored v are the last candidate's
     }
     while (it < max_iter && !(it > 0 && tol > 0.f && res <= tol)) {
       res = pass(cur, cur, want_res);
       ++it;
+      bool reset_u = false;
+      if (relax && g.step(res, it, &reset_u) && reset_u) {
+        for (int D = tid; D < RL; D += kBT) cur[D] = D < vr ? (float)vr : 0.f;
+        __syncthreads();
+      }
     }
     if (iters_out && tid == 0) iters_out[j] = it;
 
@@ -383,7 +414,7 @@ int launch_panel_to_bf16(const float* K, int ld, void* K16, int ld16, uint64_t V
   return 1;
 }
 
-template <int NQ, int kBW, int kCPS>
+template <int NQ, int kBW, int kCPS, bool RLX>
 static int launch_block_t(const void* K16, int ld16, float expo,
                           const SourceSel& s, const Targets& t,
                           const SolveCtl& ctl, const float* u0, int64_t ldu,
@@ -400,7 +431,7 @@ static int launch_block_t(const void* K16, int ld16, float expo,
     int rows = (int)((budget - Sh::bytes(0)) / (Sh::RB + 8));
     while (rows > 0 && Sh::bytes(rows) > budget) --rows;
     if (rows < 2) return -1;
-    cudaFuncSetAttribute(solve_block_kernel<NQ, kBW, kCPS>,
+    cudaFuncSetAttribute(solve_block_kernel<NQ, kBW, kCPS, RLX>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Sh::bytes(rows));
     int sms = 0;
@@ -412,10 +443,24 @@ static int launch_block_t(const void* K16, int ld16, float expo,
   int64_t grid = (int64_t)sms_cache[dev] * kCPS;
   if (grid > t.N) grid = t.N;
   if (grid < 1) grid = 1;
-  solve_block_kernel<NQ, kBW, kCPS><<<(unsigned)grid, kBW * 32, Sh::bytes(rows), st>>>(
+  solve_block_kernel<NQ, kBW, kCPS, RLX><<<(unsigned)grid, kBW * 32, Sh::bytes(rows), st>>>(
       static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr,
-      t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows, ctl.omega, out);
+      t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows, ctl.omega,
+      ctl.vstate, out);
   return 1;
+}
+
+// Over-relaxed solves (omega != 1) run the instantiation that keeps each
+// word's v; the plain one compiles without that state.
+template <int NQ, int kBW, int kCPS>
+static int launch_block_r(const void* K16, int ld16, float expo, const SourceSel& s,
+                          const Targets& t, const SolveCtl& ctl, const float* u0,
+                          int64_t ldu, double* out, cudaStream_t st) {
+  if (ctl.omega != 1.f) {
+    if (!ctl.vstate) return -1;
+    return launch_block_t<NQ, kBW, kCPS, true>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+  }
+  return launch_block_t<NQ, kBW, kCPS, false>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
 }
 
 // Launch shapes the autotuner chooses from (warps per CTA, CTAs per SM).
@@ -437,10 +482,10 @@ static int launch_nq_default(const void* K16, int ld16, float expo, const Source
                              const Targets& t, const SolveCtl& ctl, const float* u0,
                              int64_t ldu, double* out, cudaStream_t st, int shape) {
   switch (shape) {
-    case 0: return launch_block_t<NQ, 4, 4>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
-    case 1: return launch_block_t<NQ, 8, 2>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
-    case 2: return launch_block_t<NQ, 16, 1>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
-    default: return launch_block_t<NQ, W, C>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    case 0: return launch_block_r<NQ, 4, 4>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    case 1: return launch_block_r<NQ, 8, 2>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    case 2: return launch_block_r<NQ, 16, 1>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
+    default: return launch_block_r<NQ, W, C>(K16, ld16, expo, s, t, ctl, u0, ldu, out, st);
   }
 }
 

@@ -104,7 +104,8 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                 const int64_t* __restrict__ col_ptr, const uint2* __restrict__ ent,
                 const int32_t* __restrict__ order, int64_t N, int max_iter, float tol,
                 int* __restrict__ iters_out, const float* __restrict__ u0, int64_t ldu,
-                int cap, float omega, double* __restrict__ out) {
+                int cap, float omega, float* __restrict__ vstate,
+                double* __restrict__ out) {
   using Sh = TcShape<NQ>;
   constexpr int RL = Sh::RL, RP = Sh::RP, KT = Sh::KT, DPW = Sh::DPW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -128,6 +129,11 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       if (tid == 0) out[j] = __longlong_as_double(0x7ff8000000000000ll);
       continue;
     }
+    // Over-relaxation of both half-steps (vstate: each word's previous v).
+    const bool relax = vstate != nullptr;
+    RelaxGuard g;
+    g.init(omega);
+    float resv = 0.f;  // this thread's c-side residual of the current pass
     const int RT = (n + 15) >> 4, npad = RT << 4;
     const bool warm = u0 != nullptr && max_iter > 0;
 
@@ -212,18 +218,37 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     // One pass: u from `src` -> new u into `dst` (may alias); returns the
     // marginal residual of `src` (CTA-uniform) when want_res.
     auto pass = [&](const float* src, float* dst, bool want_res) -> float {
+      // Previous v of this thread's first rows, loaded before the products
+      // (off the s -> v critical path).
+      float vp[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = tid + i * kTT;
+        vp[i] = (relax && !g.vfirst && k < n) ? vstate[b + k] : 0.f;
+      }
       split_u(src);
       __syncthreads();
       product_s();
       __syncthreads();
-      for (int k = tid; k < npad; k += kTT) {
+      resv = 0.f;
+      auto row_v = [&](int k, float vold) {
         const float s = sS[k] + sS[cap + k] + sS[2 * cap + k] + sS[3 * cap + k];
         __nv_bfloat16 h, m, l;
-        split3(weight(sC[k], s), h, m, l);
+        // padding rows (k >= n) have c = 0: v = 0 and no state touched
+        split3(relax ? relaxed_v_pre(sC[k], s, vold, vstate + b + k, g.vfirst, g.omega, resv)
+                     : weight(sC[k], s),
+               h, m, l);
         sV[k] = h;
         sV[cap + k] = m;
         sV[2 * cap + k] = l;
+      };
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = tid + i * kTT;
+        if (k < npad) row_v(k, vp[i]);
       }
+      for (int k = tid + 4 * kTT; k < npad; k += kTT)
+        row_v(k, (relax && !g.vfirst && k < n) ? vstate[b + k] : 0.f);
       __syncthreads();
       // x = K^T v: this warp's dimension tiles, all row tiles.
       float c[DPW][4];
@@ -246,7 +271,7 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
 #pragma unroll
         for (int t = 0; t < DPW; ++t) mma_bf16(c[t], a[t], b0, b1);
       }
-      float res = 0.f;
+      float res = resv;
 #pragma unroll
       for (int t = 0; t < DPW; ++t) {
         const int dt = warp + kTW * t;
@@ -262,7 +287,7 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
               const float rvD = __ldg(&rinv[D]);
               const float uo = src[D];
               res += fabsf(uo * x - __frcp_rn(rvD));
-              dst[D] = relaxed_update(uo, __frcp_rn(rvD * x), omega);
+              dst[D] = relaxed_update(uo, __frcp_rn(rvD * x), g.omega);
             } else {
               dst[D] = 0.f;
             }
@@ -286,7 +311,7 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     float* cur = ubufA;
     int it = 0;
     float res = 0.f;
-    const bool want_res = tol > 0.f;
+    const bool want_res = tol > 0.f || relax;
     if (warm) {
       const float rc = pass(ubufA, ubufA, true);
       const float rwm = pass(ubufB, ubufB, true);
@@ -294,10 +319,16 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       cur = use_warm ? ubufB : ubufA;
       res = use_warm ? rwm : rc;
       it = 1;
+      g.vfirst = true;  // the stored v are the last candidate's
     }
     while (it < max_iter && !(it > 0 && tol > 0.f && res <= tol)) {
       res = pass(cur, cur, want_res);
       ++it;
+      bool reset_u = false;
+      if (relax && g.step(res, it, &reset_u) && reset_u) {
+        for (int D = tid; D < RL; D += kTT) cur[D] = D < vr ? (float)vr : 0.f;
+        __syncthreads();
+      }
     }
     if (iters_out && tid == 0) iters_out[j] = it;
 
@@ -399,7 +430,8 @@ static int launch_tc_t(const void* K16, int ld16, float expo, const SourceSel& s
   if (grid < 1) grid = 1;
   solve_tc_kernel<NQ><<<(unsigned)grid, kTT, Sh::bytes(cap), st>>>(
       static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr, t.ent,
-      t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, cap, ctl.omega, out);
+      t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, cap, ctl.omega,
+      ctl.omega != 1.f ? ctl.vstate : nullptr, out);
   return 1;
 }
 
@@ -413,6 +445,7 @@ int launch_solve_tc(const void* K16, int ld16, float expo, uint32_t vr_cap,
   if (t.N <= 0) return 0;
   if (expo == 0.f || ld16 != block_panel_width(vr_cap) || !t.order) return -1;
   if (n_long < 0 || n_long > t.N) return -1;
+  if (ctl.omega != 1.f && !ctl.vstate) return -1;
   int launches = 0;
   if (n_long > 0) {
     Targets tl = t;

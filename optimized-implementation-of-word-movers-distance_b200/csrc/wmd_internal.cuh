@@ -180,11 +180,19 @@ int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
 // u0 (optional, [N][ldu]): initial scaling per document (warm start); the
 // first update is then evaluated from both u0 and the cold start and the one
 // with the smaller marginal residual is kept.
-// omega: over-relaxation of the u update, u <- u^(1-omega) * u_hat^omega
-// with u_hat the plain update (omega = 1: the reference's iteration).  The
-// fixed point is the same; for 1 < omega < 2 slowly converging documents
-// need fewer updates (overrelaxed Sinkhorn-Knopp, Thibault, Chizat, Dossal
-// and Papadakis, 2017).
+// omega: over-relaxation of both half-steps, v <- v^(1-omega) * v_hat^omega
+// and u <- u^(1-omega) * u_hat^omega with v_hat = c / (K^T u) and u_hat the
+// plain u update (omega = 1: the reference's iteration).  The fixed point is
+// the same; for 1 < omega < 2 slowly converging documents need far fewer
+// updates (overrelaxed Sinkhorn-Knopp: Thibault, Chizat, Dossal and
+// Papadakis, 2017; Lehmann, von Renesse, Sambale and Uschmajew, 2021).  A
+// word's previous v lives in vstate[entry] (required when omega != 1, [nnz]);
+// the residual then adds the c-side marginal sum_k |v_k (K u)_k - c_k|, and a
+// per-document guard halves omega - 1 (restarting v exactly) when the
+// residual exceeds kRelaxGuard times the best one seen, and restarts the
+// document from the cold start unrelaxed (omega = 1 from then on) when the
+// residual is not finite.  Relaxation needs per-document stopping (tol > 0):
+// the caller passes omega = 1 for a fixed update count.
 struct SolveCtl {
   int max_iter = 15;
   float tol = 0.f;
@@ -192,13 +200,74 @@ struct SolveCtl {
   const float* u0 = nullptr;
   int64_t ldu = 0;
   float omega = 1.f;
+  float* vstate = nullptr;
 };
+
+constexpr float kRelaxGuard = 100.f;
 
 // The relaxed update of one scaling entry (see SolveCtl::omega).
 __device__ __forceinline__ float relaxed_update(float u_old, float u_hat, float omega) {
   if (omega == 1.f) return u_hat;
   return u_old * exp2f(omega * __log2f(u_hat / u_old));
 }
+
+// v of one target word under over-relaxation: v_hat = c / s relaxed against
+// the word's previous v (kept in *slot); exactly v_hat on a document's first
+// pass or after a guard reset.  Adds |v s - c| to resv.  Padding words
+// (c = 0) give 0 and touch nothing.
+__device__ __forceinline__ float relaxed_v(float c, float s, float* slot, bool first,
+                                           float omega, float& resv) {
+  if (c == 0.f) return 0.f;
+  const float vh = __fdividef(c, s);
+  const float v = first ? vh : relaxed_update(*slot, vh, omega);
+  *slot = v;
+  resv += fabsf(v * s - c);
+  return v;
+}
+// The same with the previous v already loaded (vold, ignored when first):
+// kernels prefetch it with the word's row, off the s -> v critical path.
+__device__ __forceinline__ float relaxed_v_pre(float c, float s, float vold, float* slot,
+                                               bool first, float omega, float& resv) {
+  if (c == 0.f) return 0.f;
+  const float vh = __fdividef(c, s);
+  const float v = first ? vh : relaxed_update(vold, vh, omega);
+  *slot = v;
+  resv += fabsf(v * s - c);
+  return v;
+}
+
+// Per-document over-relaxation guard (uniform over the threads of a
+// document).  Returns true when it reset: omega stepped halfway to 1, v to
+// restart exactly; *reset_u when the residual was not finite.
+struct RelaxGuard {
+  float omega, best;
+  bool vfirst;
+  __device__ __forceinline__ void init(float om) {
+    omega = om;
+    best = __int_as_float(0x7f800000);
+    vfirst = true;
+  }
+  __device__ __forceinline__ bool step(float res, int it, bool* reset_u) {
+    *reset_u = false;
+    vfirst = false;
+    if (omega == 1.f) return false;
+    if (!isfinite(res)) {  // diverged: cold start, plain iteration
+      omega = 1.f;
+      vfirst = true;
+      *reset_u = true;
+      return true;
+    }
+    if (it > 2 && res > kRelaxGuard * best) {
+      omega = 1.f + 0.5f * (omega - 1.f);
+      if (omega < 1.01f) omega = 1.f;
+      best = __int_as_float(0x7f800000);
+      vfirst = true;
+      return true;
+    }
+    best = fminf(best, res);
+    return false;
+  }
+};
 
 // Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
 // target document.  Returns launches issued (-1 on unsupported vr_cap).

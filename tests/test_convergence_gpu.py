@@ -66,3 +66,33 @@ def test_over_relaxation_same_fixed_point_fewer_updates(wmd, synth, oracle_mod, 
     with pytest.raises(wmd.WMDError):
         eng.set_relaxation(2.0)
     eng.close()
+
+
+@pytest.mark.parametrize("vr,prec", [(32, "fp32"), (300, "bf16"), (128, "bf16")])
+def test_over_relaxation_guard_keeps_aggressive_omega_safe(wmd, synth, oracle_mod, vr, prec):
+    """Both half-steps relaxed at omega = 1.95, where the plain relaxed
+    iteration diverges on wide sources: the per-document guard steps omega
+    back, every finished document stays within 1e-4 of the converged FP64
+    oracle.  Without a tolerance (a fixed update count) relaxation does not
+    apply: the results are the reference iteration's, bit for bit."""
+    p = synth.case(4000, 300, 200, vr, 8, 200, 60, 700 + vr)
+    conv = oracle_mod.sinkhorn_converged(p.r, p.vecs.astype(np.float64), p.col_ptr,
+                                         p.row_inds, p.vals, p.lam, tol=1e-10,
+                                         max_iter_cap=50000)[0]
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.set_solve_precision(prec)
+    eng.set_tolerance(1e-5)
+    eng.set_relaxation(1.95)
+    got = eng.query(p.r, p.lam, 5000)
+    it = eng.last_iterations()
+    done = it < 5000
+    assert done.mean() > 0.9
+    assert np.all(np.isfinite(got))
+    assert rel_err(got[done], conv[done]).max() <= 1e-4
+    eng.set_tolerance(0.0)
+    fixed = eng.query(p.r, p.lam, 40)
+    eng.set_relaxation(1.0)
+    np.testing.assert_array_equal(fixed, eng.query(p.r, p.lam, 40))
+    eng.close()
