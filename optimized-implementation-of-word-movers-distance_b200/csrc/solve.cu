@@ -140,12 +140,16 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   // 8 distinct bank groups.
   const int key = lane & 7;
 
-  // Dimensions this lane finalises after the transpose: 32*qq + lane.
+  // Dimensions this lane finalises after the transpose: 32*qq + own, with
+  // own = 2 (lane % 16) + lane / 16 when the slot sums run in pairs
+  // (LPW < 32), else own = lane.
+  constexpr bool kPairSum = LPW < 32;
+  const int own = kPairSum ? 2 * (lane & 15) + (lane >> 4) : lane;
   float rv[LPW], rw[LPW];  // 1/r_i and r_i
   unsigned dmask = 0;
 #pragma unroll
   for (int qq = 0; qq < LPW; ++qq) {
-    const int D = 32 * qq + lane;
+    const int D = 32 * qq + own;
     const bool ok = D < vr;
     rv[qq] = ok ? rinv[D] : 0.f;
     rw[qq] = ok ? __frcp_rn(rv[qq]) : 0.f;
@@ -292,8 +296,12 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       }
     };
     // Sum the x slices of all word slots: lane writes its 32 values as row
-    // `lane` of a 32x32 buffer (chunk-swizzled), then lane L sums column L for
-    // each of its LPW dimension groups: tot[qq] is dimension 32*qq + L.
+    // `lane` of a 32x32 buffer (chunk-swizzled), then each lane sums, for
+    // each of its LPW dimension groups, the slots' values of its dimension.
+    // Paired form (LPW < 32): lanes L and L ^ 16 sum the dimension pair
+    // (2p, 2p + 1), p = L % 16, over the two halves of the slots with 8-byte
+    // loads and packed adds, combine the halves with one shuffle, and keep
+    // dimension 2p + L / 16 (= own): tot[qq] is dimension 32*qq + own.
     auto reduce_slots = [&](const float2 (&x2)[16], float (&tot)[LPW]) {
       float4* rw = reinterpret_cast<float4*>(red + lane * 32);
 #pragma unroll
@@ -301,25 +309,48 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
         rw[t ^ key] = make_float4(x2[2 * t].x, x2[2 * t].y, x2[2 * t + 1].x,
                                   x2[2 * t + 1].y);
       __syncwarp();
+      if constexpr (kPairSum) {
+        constexpr int HALF = WPS / 2;
+        const int p = lane & 15, h = lane >> 4;
 #pragma unroll
-      for (int qq = 0; qq < LPW; ++qq) {
-        float part[WPS];
+        for (int qq = 0; qq < LPW; ++qq) {
+          float2 part[HALF];
 #pragma unroll
-        for (int gg = 0; gg < WPS; ++gg) {
-          const int row = gg * LPW + qq;
-          part[gg] = red[row * 32 + 4 * ((lane >> 2) ^ (row & 7)) + (lane & 3)];
+          for (int i = 0; i < HALF; ++i) {
+            const int row = (h * HALF + i) * LPW + qq;
+            part[i] = *reinterpret_cast<const float2*>(
+                red + row * 32 + 4 * ((p >> 1) ^ (row & 7)) + 2 * (p & 1));
+          }
+#pragma unroll
+          for (int w = HALF / 2; w >= 1; w >>= 1)
+#pragma unroll
+            for (int i = 0; i < w; ++i)
+              part[i] = make_float2(part[i].x + part[i + w].x, part[i].y + part[i + w].y);
+          const float2 o = make_float2(__shfl_xor_sync(0xffffffffu, part[0].x, 16),
+                                       __shfl_xor_sync(0xffffffffu, part[0].y, 16));
+          tot[qq] = h ? part[0].y + o.y : part[0].x + o.x;
         }
+      } else {
 #pragma unroll
-        for (int w = WPS / 2; w >= 1; w >>= 1)
+        for (int qq = 0; qq < LPW; ++qq) {
+          float part[WPS];
 #pragma unroll
-          for (int i = 0; i < w; ++i) part[i] += part[i + w];
-        tot[qq] = part[0];
+          for (int gg = 0; gg < WPS; ++gg) {
+            const int row = gg * LPW + qq;
+            part[gg] = red[row * 32 + 4 * ((lane >> 2) ^ (row & 7)) + (lane & 3)];
+          }
+#pragma unroll
+          for (int w = WPS / 2; w >= 1; w >>= 1)
+#pragma unroll
+            for (int i = 0; i < w; ++i) part[i] += part[i + w];
+          tot[qq] = part[0];
+        }
       }
       __syncwarp();
     };
     auto broadcast_u = [&](const float (&uval)[LPW], float2 (&u2)[16]) {
 #pragma unroll
-      for (int qq = 0; qq < LPW; ++qq) ubuf[32 * qq + lane] = uval[qq];
+      for (int qq = 0; qq < LPW; ++qq) ubuf[32 * qq + own] = uval[qq];
       __syncwarp();
       const float4* ub = reinterpret_cast<const float4*>(ubuf + 32 * q);
 #pragma unroll
@@ -398,7 +429,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
 #pragma unroll
       for (int qq = 0; qq < LPW; ++qq) {
         const bool ok = (dmask >> qq) & 1u;
-        const float uo = ubuf[32 * qq + lane];
+        const float uo = ubuf[32 * qq + own];
         if (want_res && ok) res += fabsf(uo * tot[qq] - rw[qq]);
         unew[qq] = ok ? relaxed_update(uo, __frcp_rn(rv[qq] * tot[qq]), RLX ? rg.omega : omega)
                       : 0.f;
@@ -420,7 +451,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       const float rc = step(uc, true);
 #pragma unroll
       for (int qq = 0; qq < LPW; ++qq)
-        uval[qq] = ((dmask >> qq) & 1u) ? __ldg(&u0[j * ldu + 32 * qq + lane]) : 0.f;
+        uval[qq] = ((dmask >> qq) & 1u) ? __ldg(&u0[j * ldu + 32 * qq + own]) : 0.f;
       broadcast_u(uval, u2);
       const float rwm = step(uw, true);
       const bool use_warm = isfinite(rwm) && !(rc < rwm);
