@@ -563,6 +563,10 @@ def ours(a, rank, world, local):
     if not max_rel <= tol:
         raise SystemExit(f"bench: result check failed, max rel err {max_rel:.3e}")
 
+    # The timed steps run without the engine's per-stage events: recorded
+    # inside the captured query graph they add ~19 us to a ~200 us step.  The
+    # stage times of the roofline come from a separate pass below.
+    eng.set_timing(False)
     sampler = ClockSampler(local)
     t_settle = time.perf_counter()
     for _ in range(a.warmup):
@@ -577,7 +581,6 @@ def ours(a, rank, world, local):
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(a.steps)]
-    stage = np.zeros((a.steps, 3))
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -586,7 +589,6 @@ def ours(a, rank, world, local):
         ev[k][0].record(stream)
         step()
         ev[k][1].record(stream)
-        stage[k] = eng.stage_times()
         with torch.cuda.stream(stream):
             flush.fill_(k & 0xFF)  # evict L2 between steps (not timed)
     torch.cuda.synchronize(dev)
@@ -595,6 +597,19 @@ def ours(a, rank, world, local):
     wall = time.perf_counter() - wall0
     clocks = sampler.stop()
     eng.check()
+    # Stage times (select / cost panel / solve) of the same step with the
+    # engine's stage events on, over separate steps after the timed region.
+    eng.set_timing(True)
+    step()
+    n_stage = min(a.steps, 20)
+    stage = np.zeros((n_stage, 3))
+    for k in range(n_stage):
+        step()
+        stage[k] = eng.stage_times()
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)
+    torch.cuda.synchronize(dev)
+    eng.set_timing(False)
     launches = eng.launch_count * a.steps
     step_ms = np.array([s.elapsed_time(e) for s, e in ev])
     tot_ms = float(step_ms.sum())
@@ -635,6 +650,10 @@ def ours(a, rank, world, local):
         "fp32_tflops": fl, "fp32_peak_tflops": fp32_peak,
         "fp32_frac": fl / fp32_peak,
         "stage_ms": {"select": sel_ms, "cdist": cd_ms, "solve": sv_ms},
+        "stage_ms_source": ("CUDA events between the stages of the same query "
+                            "(recorded inside its graph), averaged over separate "
+                            "steps after the timed region: the events add ~19 us "
+                            "to a step, so the timed steps run without them"),
         "bytes_model": "per iteration nnz*8 + nnz*v_r*4 + 2*N*v_r*4, final "
                        "nnz*8 + 2*nnz*v_r*4 + 8*N; cdist V*d*4 + 2*v_r*V*4",
         "note": ("the solve's bytes model counts K-row gathers that the kernel "
