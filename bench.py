@@ -359,10 +359,11 @@ def extras(a, wmd, p, dev):
     S = min(a.batch_sources, 512)
     rs, vrs = rs[:S], vrs[:S]
     eng = wmd.Engine(dev.index)
+    eng.set_cdist_mode("tf32x3")  # FP32-accurate cost panel for both arms
     eng.set_embeddings(p.vecs)
     eng.set_targets(cpb, rib, vab)
     batched = {"sources": S, "sum_vr": int(sum(vrs)), "docs": N,
-               "nnz": int(cpb[-1])}
+               "nnz": int(cpb[-1]), "cost_panel": "tf32x3 (FP32-accurate, tensor cores)"}
     for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
         eng.set_solve_precision(prec)
         eng.query_batch(_one_per_width(rs), p.lam, 15)
@@ -464,10 +465,11 @@ def large_vocab(wmd, dev):
     rs, vrs = synth.batched_sources(V, S, 16, 512, seed=9, cdf=cdf)
     gen = time.perf_counter() - t0
     eng = wmd.Engine(dev.index)
+    eng.set_cdist_mode("tf32x3")  # FP32-accurate cost panel for both arms
     eng.set_embeddings(E)
     eng.set_targets(cp, ri, va)
     res = {"V": V, "docs": N, "nnz": int(cp[-1]), "sources": S, "sum_vr": int(sum(vrs)),
-           "generation_seconds": gen}
+           "generation_seconds": gen, "cost_panel": "tf32x3 (FP32-accurate, tensor cores)"}
     for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
         eng.set_solve_precision(prec)
         eng.set_timing(True)
