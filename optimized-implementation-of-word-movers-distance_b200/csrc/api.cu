@@ -145,6 +145,15 @@ struct wmd_handle {
   DevBuf vstate;  // each target word's previous v (over-relaxed solves)
   // batched queries
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
+  // Second pipeline slot of the batched queries (its own stream and
+  // per-source scratch): consecutive sources alternate between the slots, so
+  // one source's solve tail overlaps the next source's cost panel and solve.
+  struct BatchSlot {
+    DevBuf sel_S, sel_nS, sel_S16, near_pairs, near_count, K, KM, K16, vstate,
+        ws_Asrc, ws_u0;
+  } slot1;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t join[2] = {nullptr, nullptr};
   // top-k
   DevBuf topk_scratch, topk_idx, topk_val;
   // learned warm start: model (FP32 parameters, folded inference form),
@@ -376,11 +385,27 @@ int64_t tc_long_count(wmd_handle* h, int ld16, int shape) {
 int launch_block_shape(wmd_handle* h, const void* K16, int ld16, float expo,
                        uint32_t vr, const SourceSel& sel, const Targets& t,
                        const SolveCtl& ctl, const float* u0, int64_t ldu,
-                       double* out, int shape) {
+                       double* out, int shape, cudaStream_t st) {
   if (shape >= 3 && shape <= 5)
-    return launch_solve_tc(K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, h->stream,
+    return launch_solve_tc(K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, st,
                            1 << (shape - 3), tc_long_count(h, ld16, shape));
-  return launch_solve_block(K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, h->stream, shape);
+  return launch_solve_block(K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, st, shape);
+}
+int launch_block_shape(wmd_handle* h, const void* K16, int ld16, float expo,
+                       uint32_t vr, const SourceSel& sel, const Targets& t,
+                       const SolveCtl& ctl, const float* u0, int64_t ldu,
+                       double* out, int shape) {
+  return launch_block_shape(h, K16, ld16, expo, vr, sel, t, ctl, u0, ldu, out, shape,
+                            h->stream);
+}
+
+// Autotuner cache slot of a panel width (and whether the panel is beyond L2),
+// and whether the shape for it is settled (pinned, tuning off, or tuned).
+int block_shape_key(const wmd_handle* h, int ld16) {
+  return ((ld16 / 128 - 1) & 3) * 2 + ((size_t)h->V * ld16 * 2 > (64u << 20) ? 1 : 0);
+}
+bool block_shape_known(const wmd_handle* h, int ld16) {
+  return h->forced_shape != -2 || !h->autotune || h->blk_shape[block_shape_key(h, ld16)] != -2;
 }
 
 // Launch shape of the block solve for this panel: cached per (width, panel
@@ -392,7 +417,7 @@ int block_shape_for(wmd_handle* h, const void* K16, int ld16, float expo,
                     uint32_t vr, const SourceSel& sel, const Targets& t,
                     const SolveCtl& ctl, double* out, bool can_sync) {
   if (h->forced_shape != -2) return h->forced_shape;
-  const int key = ((ld16 / 128 - 1) & 3) * 2 + ((size_t)h->V * ld16 * 2 > (64u << 20) ? 1 : 0);
+  const int key = block_shape_key(h, ld16);
   if (h->blk_shape[key] != -2) return h->blk_shape[key];
   if (!h->autotune || !can_sync) return -1;
   SolveCtl c2 = ctl;
@@ -782,6 +807,29 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   const unsigned near_cap = (unsigned)std::min<uint64_t>((uint64_t)V * vr_max, 1u << 20);
   CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
   CK(h->near_count.ensure(sizeof(unsigned)));
+  // Two pipeline slots when there is more than one source: slot 1 mirrors
+  // slot 0's per-source scratch on its own stream.
+  const bool overlap = S > 1;
+  if (overlap) {
+    wmd_handle::BatchSlot& b1 = h->slot1;
+    if (!h->stream2) CK(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->join)
+      if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CK(b1.sel_S.ensure((size_t)vr_max * d * sizeof(float)));
+    CK(b1.sel_nS.ensure((size_t)vr_max * sizeof(float)));
+    CK(b1.K.ensure((size_t)V * ld_max * sizeof(float)));
+    if (need_km) CK(b1.KM.ensure((size_t)V * ld_max * sizeof(float)));
+    if (ld16_max) CK(b1.K16.ensure((size_t)V * ld16_max * 2));
+    if (h->omega != 1.f)
+      CK(b1.vstate.ensure((size_t)std::max<uint64_t>(h->nnz, 1) * sizeof(float)));
+    if (ws) {
+      CK(b1.ws_Asrc.ensure((size_t)vr_max * kWsH * sizeof(float)));
+      CK(b1.ws_u0.ensure((size_t)std::max<uint64_t>(N, 1) * ld_max * sizeof(float)));
+    }
+    CK(b1.near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
+    CK(b1.near_count.ensure(sizeof(unsigned)));
+    if (tcm) CK(b1.sel_S16.ensure((size_t)vr_max * dp * 2));
+  }
   int launches = 0;
   if (tcm) {
     const int fmt = bf16 ? 1 : 2;
@@ -808,20 +856,38 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   t.nnz = (int64_t)h->nnz;
   if (h->timing)
     for (int i = 0; i < 3; ++i) CK(cudaEventRecord(h->ev[i], h->stream));
+  if (overlap) {  // slot 1 starts after the uploads above
+    CK(cudaEventRecord(h->join[0], h->stream));
+    CK(cudaStreamWaitEvent(h->stream2, h->join[0], 0));
+  }
   for (uint64_t s = 0; s < S; ++s) {
     const uint64_t off = src_ptr[s];
     const uint32_t vr = vrs[s];
     const int ld = (int)(((vr ? vr : 1) + 3u) & ~3u);
+    // this source's pipeline slot: stream and scratch
+    const bool in1 = overlap && (s & 1);
+    cudaStream_t sst = in1 ? h->stream2 : h->stream;
+    DevBuf& bS = in1 ? h->slot1.sel_S : h->sel_S;
+    DevBuf& bnS = in1 ? h->slot1.sel_nS : h->sel_nS;
+    DevBuf& bS16 = in1 ? h->slot1.sel_S16 : h->sel_S16;
+    DevBuf& bNP = in1 ? h->slot1.near_pairs : h->near_pairs;
+    DevBuf& bNC = in1 ? h->slot1.near_count : h->near_count;
+    DevBuf& bK = in1 ? h->slot1.K : h->K;
+    DevBuf& bK16 = in1 ? h->slot1.K16 : h->K16;
+    DevBuf& bVS = in1 ? h->slot1.vstate : h->vstate;
+    DevBuf& bAs = in1 ? h->slot1.ws_Asrc : h->ws_Asrc;
+    DevBuf& bU0 = in1 ? h->slot1.ws_u0 : h->ws_u0;
+    float* KMs = need_km ? (in1 ? h->slot1.KM : h->KM).as<float>() : nullptr;
     SourceSel sel;
     sel.ids = h->b_ids.as<uint32_t>() + off;
     sel.rinv = h->b_rinv.as<float>() + off;
-    sel.S = h->sel_S.as<float>();
-    sel.nS = h->sel_nS.as<float>();
+    sel.S = bS.as<float>();
+    sel.nS = bnS.as<float>();
     sel.vr = h->b_vr.as<uint32_t>() + s;
     sel.cap = vr;
     NearList near;
-    near.pairs = h->near_pairs.as<uint2>();
-    near.count = h->near_count.as<unsigned>();
+    near.pairs = bNP.as<uint2>();
+    near.count = bNC.as<unsigned>();
     near.cap = near_cap;
     near.E32 = h->E32.as<float>();
     near.S32 = sel.S;
@@ -829,55 +895,68 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     launches += launch_gather_sources(sel.ids, (int)vr, h->E32.as<float>(),
                                       h->nE.as<float>(), d, sel.S, sel.nS,
                                       tcm ? h->E16.p : nullptr,
-                                      tcm ? h->sel_S16.p : nullptr, dp, h->stream);
-    CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
+                                      tcm ? bS16.p : nullptr, dp, sst);
+    CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), sst));
     if (tcm || x3) {
       const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
-                                     h->E16.p, h->sel_S16.p, h->E32.as<float>(),
+                                     h->E16.p, bS16.p, h->E32.as<float>(),
                                      h->nE.as<float>(), V, d, sel, expo,
-                                     h->K.as<float>(), KMp, ld, near,
-                                     h->err_dev.as<unsigned>(), h->sms, h->stream);
-      if (lc < 0)
+                                     bK.as<float>(), KMs, ld, near,
+                                     h->err_dev.as<unsigned>(), h->sms, sst);
+      if (lc < 0) {
+        if (overlap) cudaStreamSynchronize(h->stream2);
         return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable");
+      }
       launches += lc;
     } else {
       launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d,
-                                    sel, expo, h->K.as<float>(), KMp, ld, near,
-                                    h->stream);
+                                    sel, expo, bK.as<float>(), KMs, ld, near, sst);
     }
-    launches += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
-                                  h->nE.as<float>(), sel.nS, sel.vr, h->sms,
-                                  h->stream);
+    launches += launch_near_fixup(near, expo, bK.as<float>(), KMs, ld, V,
+                                  h->nE.as<float>(), sel.nS, sel.vr, h->sms, sst);
     SolveCtl ctl;
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->b_iters.as<int>() + s * N;
     ctl.omega = h->tol > 0.f ? h->omega : 1.f;  // relaxation needs stopping
-    ctl.vstate = ctl.omega != 1.f ? h->vstate.as<float>() : nullptr;
+    ctl.vstate = ctl.omega != 1.f ? bVS.as<float>() : nullptr;
     if (ws && vr > 0) {
       launches += launch_ws_init(ws_layout((int)d), h->ws_folded.as<float>(),
                                  h->ws_params.as<float>(), sel.S, sel.rinv, (int)vr,
-                                 h->K.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
-                                 h->ws_Asrc.as<float>(), h->ws_u0.as<float>(), ld,
-                                 h->err_dev.as<unsigned>(), h->sms, h->stream);
-      ctl.u0 = h->ws_u0.as<float>();
+                                 bK.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
+                                 bAs.as<float>(), bU0.as<float>(), ld,
+                                 h->err_dev.as<unsigned>(), h->sms, sst);
+      ctl.u0 = bU0.as<float>();
       ctl.ldu = ld;
     }
-    const int ld16 = h->prec == WMD_SOLVE_BF16 && !KMp ? block_panel_width(vr) : 0;
+    const int ld16 = h->prec == WMD_SOLVE_BF16 && !KMs ? block_panel_width(vr) : 0;
     int ls;
     if (ld16) {
-      launches += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V,
-                                       sel.vr, h->sms, h->stream);
-      const int shape = block_shape_for(h, h->K16.p, ld16, expo, vr, sel, t, ctl,
+      launches += launch_panel_to_bf16(bK.as<float>(), ld, bK16.p, ld16, V, sel.vr,
+                                       h->sms, sst);
+      if (overlap && !block_shape_known(h, ld16)) {
+        // the autotuner times its candidates on the handle's stream: nothing
+        // else may run meanwhile, and this slot's panel must be complete
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaStreamSynchronize(h->stream2));
+      }
+      const int shape = block_shape_for(h, bK16.p, ld16, expo, vr, sel, t, ctl,
                                         h->b_out.as<double>() + s * N, true);
-      ls = launch_block_shape(h, h->K16.p, ld16, expo, vr, sel, t, ctl, ctl.u0, ctl.ldu,
-                              h->b_out.as<double>() + s * N, shape);
+      ls = launch_block_shape(h, bK16.p, ld16, expo, vr, sel, t, ctl, ctl.u0, ctl.ldu,
+                              h->b_out.as<double>() + s * N, shape, sst);
     } else {
-      ls = launch_solve(h->K.as<float>(), KMp, ld, expo, vr, sel, t, ctl,
-                        h->b_out.as<double>() + s * N, h->stream);
+      ls = launch_solve(bK.as<float>(), KMs, ld, expo, vr, sel, t, ctl,
+                        h->b_out.as<double>() + s * N, sst);
     }
-    if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "a source has more than 1024 words");
+    if (ls < 0) {
+      if (overlap) cudaStreamSynchronize(h->stream2);
+      return fail(WMD_ERR_UNSUPPORTED, "a source has more than 1024 words");
+    }
     launches += ls;
+  }
+  if (overlap) {  // the results wait for both slots
+    CK(cudaEventRecord(h->join[1], h->stream2));
+    CK(cudaStreamWaitEvent(h->stream, h->join[1], 0));
   }
   if (h->timing) CK(cudaEventRecord(h->ev[3], h->stream));
   CK(cudaGetLastError());
@@ -1129,6 +1208,12 @@ wmd_status wmd_destroy(wmd_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   for (int i = 0; i < 4; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->stream2) {
+    cudaStreamSynchronize(h->stream2);
+    cudaStreamDestroy(h->stream2);
+  }
+  for (cudaEvent_t e : h->join)
+    if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return WMD_OK;
