@@ -40,11 +40,24 @@ namespace wmd {
 
 // Launch shape (warps per CTA, CTAs per SM) and arithmetic form: build-time
 // tuning knobs, the defaults being the measured best on B200.
+// Wide sources (LPW > 1): 4 warps x 2 CTAs per SM, two staged rounds in
+// flight.  v_r <= 32 (LPW = 1): one-warp CTAs, eight per SM, one round in
+// flight -- the same occupancy, measured 6 % faster there and 12-27 % slower
+// for the wide instantiations.
 #ifndef WMD_SOLVE_WARPS
 #define WMD_SOLVE_WARPS 4
 #endif
 #ifndef WMD_SOLVE_CTAS_PER_SM
 #define WMD_SOLVE_CTAS_PER_SM 2
+#endif
+#ifndef WMD_SOLVE_WARPS_1
+#define WMD_SOLVE_WARPS_1 1
+#endif
+#ifndef WMD_SOLVE_CTAS_PER_SM_1
+#define WMD_SOLVE_CTAS_PER_SM_1 8
+#endif
+#ifndef WMD_SOLVE_UNROLL_1
+#define WMD_SOLVE_UNROLL_1 1
 #endif
 #ifndef WMD_SOLVE_PACKED_FMA
 #define WMD_SOLVE_PACKED_FMA 1
@@ -60,7 +73,14 @@ namespace wmd {
 #endif
 
 namespace {
-constexpr int kWarps = WMD_SOLVE_WARPS;  // warps per CTA
+// Launch shape per lane layout: warps per CTA, CTAs per SM, staged rounds
+// in flight per step.
+template <int LPW>
+struct SolveCfg {
+  static constexpr int kWarps = LPW == 1 ? WMD_SOLVE_WARPS_1 : WMD_SOLVE_WARPS;
+  static constexpr int kCtas = LPW == 1 ? WMD_SOLVE_CTAS_PER_SM_1 : WMD_SOLVE_CTAS_PER_SM;
+  static constexpr int kUnroll = LPW == 1 ? WMD_SOLVE_UNROLL_1 : WMD_SOLVE_UNROLL;
+};
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -110,7 +130,7 @@ struct SolveShape {
 };
 
 template <int LPW, bool FROM_KM, bool RLX>
-__global__ void __launch_bounds__(kWarps * 32, WMD_SOLVE_CTAS_PER_SM)
+__global__ void __launch_bounds__(SolveCfg<LPW>::kWarps * 32, SolveCfg<LPW>::kCtas)
 solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              float expo, const uint32_t* __restrict__ vr_dev,
              const float* __restrict__ rinv,
@@ -156,6 +176,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     dmask |= ok ? (1u << qq) : 0u;
   }
 
+  constexpr int kWarps = SolveCfg<LPW>::kWarps;
   const int64_t total_warps = (int64_t)gridDim.x * kWarps;
   int64_t idx = (int64_t)blockIdx.x * kWarps + warp;
   // Pointers of the current document; the next one's are prefetched while
@@ -376,7 +397,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
         for (int t = 0; t < RR; ++t)
           axpy(reg[t], vweight(creg[t], sreg[t], t * WPS + g, oreg[t]), x2);
       }
-      constexpr int U = WMD_SOLVE_UNROLL;
+      constexpr int U = SolveCfg<LPW>::kUnroll;
       int t = 0;
       for (; t + U <= sr; t += U) {
         Row ra[U];
@@ -554,7 +575,8 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
                           const SolveCtl& ctl, double* out, cudaStream_t st) {
   using Sh = SolveShape<LPW>;
   constexpr int kMaxDev = 64;
-  constexpr int kBlocksPerSm = WMD_SOLVE_CTAS_PER_SM;
+  constexpr int kBlocksPerSm = SolveCfg<LPW>::kCtas;
+  constexpr int kWarps = SolveCfg<LPW>::kWarps;
   constexpr size_t kSmemPerSm = 227 * 1024;
   static int sms_cache[kMaxDev] = {0};
   static int srounds_cache[kMaxDev] = {0};
