@@ -283,10 +283,15 @@ class Engine:
         self.N = int(N)
 
     def set_cdist_mode(self, mode: str):
+        """Cost panel: "fp32" (CUDA cores, the default), "tf32x3" (tcgen05
+        tensor cores on the FP32 embeddings split into TF32 high + low
+        parts: FP32-accurate), "fp16" / "bf16" (16-bit operands)."""
         check(lib().wmd_set_cdist_mode(self._h, CDIST_MODES[mode]))
 
     def set_relaxation(self, omega: float = 1.0):
-        """Over-relaxed u update (1 = the reference's iteration)."""
+        """Over-relaxation of both Sinkhorn half-steps, 0 < omega < 2, with a
+        per-document guard; applies with a tolerance set (set_tolerance),
+        1 = the reference's iteration."""
         check(lib().wmd_set_relaxation(self._h, float(omega)))
 
     def set_autotune(self, enable: bool = True):
