@@ -83,3 +83,21 @@ def test_tf32x3_close_to_fp32_panel(wmd, full):
           f"vs FP64: {rel_err(x3, ref).max():.3e} / {rel_err(f32, ref).max():.3e}")
     assert d.max() <= 5e-6
     eng.close()
+
+
+@pytest.mark.parametrize("mode", ["fp32", "tf32x3", "fp16", "bf16"])
+def test_lambda_zero_reads_the_km_panel(wmd, synth, oracle_mod, mode):
+    """lambda = 0: K = 1 everywhere, so the final half-step cannot recover
+    K.*M from K and every form writes and reads the K.*M panel (single and
+    batched queries)."""
+    p = synth.case(1500, 300, 80, 24, 8, 80, 30, 901)
+    ref = oracle_mod.sinkhorn(p.r, p.vecs.astype(np.float64), p.col_ptr, p.row_inds,
+                              p.vals, 0.0, 15)
+    eng = _engine(wmd, p, mode)
+    got = eng.query(p.r, 0.0, 15)
+    tol = {"fp32": 1e-5, "tf32x3": 1e-5, "fp16": 1e-3, "bf16": 1e-2}[mode]
+    assert rel_err(got, ref).max() <= tol
+    batch = eng.query_batch([p.r, p.r], 0.0, 15)
+    np.testing.assert_array_equal(batch[0], got)
+    np.testing.assert_array_equal(batch[1], got)
+    eng.close()
