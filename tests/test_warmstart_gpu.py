@@ -133,14 +133,21 @@ def test_end_to_end_gain(wmd, synth, oracle_mod):
     cold, it_cold = eng.query_batch(held, p.lam, 5000, want_iters=True)
     eng.set_warm_start(params)
     warm, it_warm = eng.query_batch(held, p.lam, 5000, want_iters=True)
+    # the warm start combined with over-relaxation of both half-steps
+    eng.set_relaxation(1.7)
+    warm_rx, it_rx = eng.query_batch(held, p.lam, 5000, want_iters=True)
+    eng.set_relaxation(1.0)
     for q, r in enumerate(held):
         conv = oracle_mod.sinkhorn_converged(r, p.vecs.astype(np.float64), p.col_ptr,
                                              p.row_inds, p.vals, p.lam, tol=1e-9,
                                              max_iter_cap=50000)[0]
-        done = (it_warm[q] < 5000) & (it_cold[q] < 5000)
+        done = (it_warm[q] < 5000) & (it_cold[q] < 5000) & (it_rx[q] < 5000)
         assert done.mean() > 0.95
         assert rel_err(warm[q][done], conv[done]).max() <= 1e-4
         assert rel_err(cold[q][done], conv[done]).max() <= 1e-4
-    print(f"mean iterations cold {it_cold.mean():.1f} warm {it_warm.mean():.1f}")
+        assert rel_err(warm_rx[q][done], conv[done]).max() <= 1e-4
+    print(f"mean iterations cold {it_cold.mean():.1f} warm {it_warm.mean():.1f} "
+          f"warm + omega 1.7 {it_rx.mean():.1f}")
     assert it_warm.mean() < it_cold.mean()
+    assert it_rx.mean() < it_warm.mean()
     eng.close()
