@@ -178,7 +178,19 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
 
   constexpr int kWarps = SolveCfg<LPW>::kWarps;
   const int64_t total_warps = (int64_t)gridDim.x * kWarps;
-  int64_t idx = (int64_t)blockIdx.x * kWarps + warp;
+  // Persistent warps over the documents in decreasing-length order, in
+  // "snake" order: in lap p over the grid, warp w takes position
+  // p*W + w for even p and p*W + (W-1-w) for odd p, so a warp that drew one
+  // of the longest documents of a lap draws one of the shortest of the
+  // next.  A plain stride hands warp 0 the longest document of every lap
+  // (about 22 % above the mean load at the single-source workload).
+  // Positions grow strictly with p, so the loop ends at the first >= N.
+  const int64_t wid = (int64_t)blockIdx.x * kWarps + warp;
+  auto position = [&](int64_t p) -> int64_t {
+    return p * total_warps + ((p & 1) ? total_warps - 1 - wid : wid);
+  };
+  int64_t lap = 0;
+  int64_t idx = position(0);
   // Pointers of the current document; the next one's are prefetched while
   // this one is processed.
   int64_t j = 0, b = 0;
@@ -188,11 +200,11 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     b = col_ptr[j];
     n = (int)(col_ptr[j + 1] - b);
   }
-  for (; idx < N; idx += total_warps) {
+  for (; idx < N; idx = position(++lap)) {
     RelaxGuard rg;  // over-relaxation of this document (RLX instantiations)
     rg.init(omega);
     float resv = 0.f;  // this lane's c-side residual of the current pass
-    const int64_t nidx = idx + total_warps;
+    const int64_t nidx = position(lap + 1);
     int64_t jn = 0;
     if (nidx < N) jn = order ? (int64_t)__ldg(&order[nidx]) : nidx;
     const int rounds = (n + WPS - 1) / WPS;
