@@ -245,14 +245,28 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def traffic_from_profiles(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
-    path = os.path.join(REPO, "profiles", "dram_traffic.json")
+def traffic_from_profiles(kernel: str, kind: str = "dram"):
+    """Bytes per launch of `kernel` from the committed ncu summaries:
+    kind "dram" (dram__bytes_read.sum + dram__bytes_write.sum) or "l2"
+    (lts__t_bytes.sum)."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel)
+            return json.load(f).get(kernel, {}).get(kind)
     except Exception:
         return None
+
+
+def probe_roofline(wmd, device: int):
+    """Measured L2 read bandwidth (GB/s) and FP32 FMA rate (TFLOP/s) of this
+    GPU, from the library's probe kernels (CUDA events)."""
+    import ctypes
+    gbs, tf = ctypes.c_double(), ctypes.c_double()
+    st = wmd.lib().wmd_probe_roofline(int(device), 64 << 20, ctypes.byref(gbs),
+                                      ctypes.byref(tf))
+    if st != 0:
+        return None, None
+    return gbs.value, tf.value
 
 
 def measured_peaks():
@@ -623,6 +637,7 @@ def ours(a, rank, world, local):
     value = pairs / (tot_ms / 1e3)
 
     # Dominant kernel + roofline (per-launch averages over the timed steps).
+    l2_peak, fp32_peak_meas = probe_roofline(wmd, local)
     sel_ms, cd_ms, sv_ms = stage.mean(axis=0)
     nnz, vr, V, d, N = p.nnz, W["v_r"], W["V"], W["d"], p.N
     it = W["max_iter"]
@@ -633,38 +648,67 @@ def ours(a, rank, world, local):
     cdist_flops = 2 * vr * V * d
     peak_hbm, peak_src = measured_peaks()
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-    cd_name = "cdist_fp32_kernel" if a.cdist == "fp32" else "cdist_tc_kernel"
+    fp32_nominal = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
+    cd_name = {"fp32": "cdist_fp32_kernel", "tf32x3": "cdist_tc_kernel_tf32x3"}.get(
+        a.cdist, "cdist_tc_kernel")
     if a.cdist in ("fp16", "bf16"):
         cdist_bytes = V * ((d + 7) // 8 * 8) * 2 + 2 * vr * V * 4
     dominant = "solve_kernel" if sv_ms >= cd_ms else cd_name
     if dominant == "solve_kernel":
-        ach = solve_bytes / (sv_ms * 1e-3) / 1e9
-        fl = solve_flops / (sv_ms * 1e-3) / 1e12
+        # The solve gathers each document's K rows once from the L2-resident
+        # panel and reuses them from registers / shared memory for all 16
+        # passes: neither HBM nor L2 bandwidth binds it, the FP32 FMA rate
+        # does (dot product + update per entry per pass).
+        t_s = sv_ms * 1e-3
+        fl = solve_flops / t_s / 1e12
+        peak_fp32 = fp32_peak_meas or fp32_nominal
+        dram = traffic_from_profiles("solve_kernel", "dram")
+        l2b = traffic_from_profiles("solve_kernel", "l2")
+        roofline = {
+            "bound": "fp32", "kernel": dominant, "achieved": fl,
+            "peak": peak_fp32, "unit": "TFLOP/s", "frac": fl / peak_fp32,
+            "peak_source": ("measured: wmd_probe_roofline packed-FMA kernel on this "
+                            "GPU" if fp32_peak_meas else
+                            "nominal 148 SMs x 128 FMA/clk at the sampled clock"),
+            "flops_model": "4*nnz*v_r*(max_iter+1): dot product + update per "
+                           "entry per pass",
+            "traffic": dram,
+            "hbm": {"bytes": dram,
+                    "achieved_gbs": dram / t_s / 1e9 if dram else None,
+                    "peak_gbs": peak_hbm,
+                    "frac": dram / t_s / 1e9 / peak_hbm if dram else None,
+                    "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"},
+            "l2": {"bytes": l2b,
+                   "achieved_gbs": l2b / t_s / 1e9 if l2b else None,
+                   "peak_gbs": l2_peak,
+                   "frac": l2b / t_s / 1e9 / l2_peak if (l2b and l2_peak) else None,
+                   "peak_source": "measured: wmd_probe_roofline L2-resident read "
+                                  "kernel on this GPU"},
+            "bytes_model": {"bytes": solve_bytes,
+                            "gbs": solve_bytes / t_s / 1e9,
+                            "what": "per iteration nnz*8 + nnz*v_r*4 + 2*N*v_r*4, "
+                                    "final nnz*8 + 2*nnz*v_r*4 + 8*N: every K-row "
+                                    "gather counted each pass, most of them served "
+                                    "from registers / shared memory"},
+            "fp32_nominal_tflops": fp32_nominal,
+            "stage_ms": {"select": sel_ms, "cdist": cd_ms, "solve": sv_ms},
+        }
     else:
-        ach = cdist_bytes / (cd_ms * 1e-3) / 1e9
-        fl = cdist_flops / (cd_ms * 1e-3) / 1e12
-    roofline = {
-        "bound": "hbm", "kernel": dominant, "achieved": ach, "peak": peak_hbm,
-        "unit": "GB/s", "frac": ach / peak_hbm,
-        "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
-        "traffic": traffic_from_profiles(dominant),
-        "fp32_tflops": fl, "fp32_peak_tflops": fp32_peak,
-        "fp32_frac": fl / fp32_peak,
-        "stage_ms": {"select": sel_ms, "cdist": cd_ms, "solve": sv_ms},
-        "stage_ms_source": ("CUDA events between the stages of the same query "
-                            "(recorded inside its graph), averaged over separate "
-                            "steps after the timed region: the events add ~19 us "
-                            "to a step, so the timed steps run without them"),
-        "bytes_model": "per iteration nnz*8 + nnz*v_r*4 + 2*N*v_r*4, final "
-                       "nnz*8 + 2*nnz*v_r*4 + 8*N; cdist V*d*4 + 2*v_r*V*4",
-        "note": ("the solve's bytes model counts K-row gathers that the kernel "
-                 "serves from L2 and on-chip storage (the panel is L2-resident, "
-                 "a document's rows are reused across all passes), so frac > 1 "
-                 "is expected; DRAM traffic per launch is `traffic` (ncu), and "
-                 "the binding limit is FP32 issue/latency: fp32_frac")
-                if dominant == "solve_kernel" else None,
-    }
+        t_c = cd_ms * 1e-3
+        ach = cdist_bytes / t_c / 1e9
+        roofline = {
+            "bound": "hbm", "kernel": dominant, "achieved": ach, "peak": peak_hbm,
+            "unit": "GB/s", "frac": ach / peak_hbm,
+            "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": traffic_from_profiles(dominant, "dram"),
+            "bytes_model": "V*d*b_E + 2*v_r*V*4",
+            "tflops": cdist_flops / t_c / 1e12,
+            "stage_ms": {"select": sel_ms, "cdist": cd_ms, "solve": sv_ms},
+        }
+    roofline["stage_ms_source"] = (
+        "CUDA events between the stages of the same query (recorded inside its "
+        "graph), averaged over separate steps after the timed region: the "
+        "events add ~19 us to a step, so the timed steps run without them")
 
     # e2e through the drop-in C ABI with pinned host buffers.
     vecs_h = torch.from_numpy(p.vecs.astype(np.float64)).pin_memory()
@@ -742,8 +786,8 @@ def ours(a, rank, world, local):
                     "h2d_input_bytes": h2d_full,
                     "api": ("wmd_sinkhorn_fused_csc (drop-in, pinned host "
                             "buffers: the GPU reads only the embedding rows of "
-                            "words in the targets or the source; FP32 "
-                            "CUDA-core cost panel)"),
+                            "words in the targets or the source; FP32-accurate "
+                            "split-TF32 tcgen05 cost panel)"),
                     "h2d_gbs": e2e_pcie_gbs,
                     "resident_corpus_value": res_value,
                     "resident_corpus_h2d_bytes_per_step": p.V * 8,

@@ -45,7 +45,10 @@ typedef enum wmd_status {
   WMD_ERR_OUT_OF_MEMORY = 3,
   WMD_ERR_CUDA = 4,          /* CUDA runtime error; see wmd_last_error() */
   WMD_ERR_NO_DEVICE = 5,
-  WMD_ERR_UNSUPPORTED = 6    /* option not available on this device/build */
+  WMD_ERR_UNSUPPORTED = 6,   /* option not available on this device/build */
+  WMD_ERR_DEVICE_TIMEOUT = 7 /* a bounded device-side wait gave up; the
+                                kernel returned early, results are invalid,
+                                the CUDA context stays usable */
 } wmd_status;
 
 /* Word-major target matrix; field-for-field the reference's
@@ -252,8 +255,28 @@ wmd_status wmd_set_tolerance(wmd_handle* h, double tol);
 wmd_status wmd_last_iterations(wmd_handle* h, int* iters);
 
 /* Synchronises the handle's stream and reports device-side validation
- * failures of the calls issued since the previous check. */
+ * failures of the calls issued since the previous check
+ * (WMD_ERR_INVALID_INPUT), or WMD_ERR_DEVICE_TIMEOUT when a bounded
+ * device-side wait gave up. */
 wmd_status wmd_check(wmd_handle* h);
+
+/* Failure-path self-test, no reference counterpart (the reference has no
+ * device waits).  Launches, on the handle's stream, one thread that waits on
+ * a device barrier nothing ever completes, through the same bounded wait the
+ * tensor-core kernels use, with a limit of limit_ns (1e3 .. 2e9) instead of
+ * their 2 s.  The wait gives up, flags the handle's error word and returns;
+ * the next wmd_check() reports WMD_ERR_DEVICE_TIMEOUT and the handle stays
+ * usable.  Hangs nothing and faults nothing. */
+wmd_status wmd_selftest_bounded_wait(wmd_handle* h, uint64_t limit_ns);
+
+/* Roofline probes, no reference counterpart: the measured L2 read bandwidth
+ * (16-byte loads over an L2-resident buffer of l2_bytes, 1 MiB .. 96 MiB,
+ * GB/s) and FP32 FMA rate (packed FMAs on registers, TFLOP/s) of `device`,
+ * timed with CUDA events.  The denominators of the iteration kernels'
+ * roofline, which neither HBM nor the tensor cores bound.  Allocates its own
+ * buffers; not part of any solve. */
+wmd_status wmd_probe_roofline(int device, uint64_t l2_bytes, double* l2_read_gbs,
+                              double* fp32_tflops);
 
 /* The handle's CUDA stream (a cudaStream_t), for event timing. */
 void* wmd_stream(wmd_handle* h);
@@ -291,16 +314,20 @@ wmd_status wmd_stage_times(wmd_handle* h, float* select_ms, float* cdist_ms,
  * entry points (FP32 cost panel) on `stream` (a cudaStream_t, NULL for the
  * default stream) and returns after synchronising it.
  *
- * Limit: the problem must fit the scratch, 2*V*round_up(vr_cap,4)*4 + V*4 +
- * nnz*8 + (N+1)*8 + vr_cap*(d+3)*4 bytes (plus about 33 KB of counters,
- * near-pair list and alignment padding) <= 64 MiB; larger problems return
- * WMD_ERR_INVALID_ARG.
+ * Limit: the problem must fit the scratch, V*round_up(vr_cap,4)*4 (twice
+ * that for lambda = 0, where the K.*M panel is stored too) + V*4 + nnz*8 +
+ * (N+1)*8 + vr_cap*(d+3)*4 bytes (plus about 33 KB of counters, near-pair
+ * list and alignment padding) <= 64 MiB; larger problems return
+ * WMD_ERR_INVALID_ARG.  vecs_dev must be 16-byte aligned when d % 4 == 0
+ * (WMD_ERR_INVALID_ARG otherwise).
  *
  * The first call on each device resolves the scratch array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture begins.  Every call on a device shares the one
- * scratch array, so calls that overlap on the GPU (other streams or host
- * threads on the same device) race: serialise them.
+ * before any stream capture begins.  The address is cached for the life of
+ * the device's primary context (do not call this again on a device after
+ * cudaDeviceReset).  Every call on a device shares the one scratch array, so
+ * calls that overlap on the GPU (other streams or host threads on the same
+ * device) race: serialise them.
  */
 wmd_status wmd_sinkhorn_noalloc(const double* r_dev, const float* vecs_dev,
                                 uint64_t V, uint64_t d,

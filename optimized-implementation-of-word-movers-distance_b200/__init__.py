@@ -450,6 +450,13 @@ class Engine:
     def check(self):
         check(lib().wmd_check(self._h))
 
+    def selftest_bounded_wait(self, limit_ns: int) -> int:
+        """Run the bounded-wait self-test (a device wait that can only end
+        through its limit) and return the status the next check reports
+        (WMD_ERR_DEVICE_TIMEOUT = 7 when the wait gave up as designed)."""
+        check(lib().wmd_selftest_bounded_wait(self._h, int(limit_ns)))
+        return int(lib().wmd_check(self._h))
+
     def set_tolerance(self, tol: float):
         """0: fixed max_iter updates (the reference); > 0: stop each document
         once its marginal residual is <= tol (max_iter becomes a cap)."""

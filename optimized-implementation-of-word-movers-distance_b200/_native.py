@@ -20,7 +20,7 @@ c_i64p = ctypes.POINTER(ctypes.c_int64)
 STATUS = {
     0: "WMD_OK", 1: "WMD_ERR_INVALID_ARG", 2: "WMD_ERR_INVALID_INPUT",
     3: "WMD_ERR_OUT_OF_MEMORY", 4: "WMD_ERR_CUDA", 5: "WMD_ERR_NO_DEVICE",
-    6: "WMD_ERR_UNSUPPORTED",
+    6: "WMD_ERR_UNSUPPORTED", 7: "WMD_ERR_DEVICE_TIMEOUT",
 }
 
 CDIST_MODES = {"fp32": 0, "bf16": 1, "fp16": 2, "tf32x3": 3}
@@ -109,6 +109,9 @@ _SIGS = [
      [ctypes.c_void_p, ctypes.c_void_p, c_u64, ctypes.c_double, ctypes.c_int,
       ctypes.c_void_p]),
     ("wmd_check", ctypes.c_int, [ctypes.c_void_p]),
+    ("wmd_selftest_bounded_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("wmd_probe_roofline", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_uint64, c_f64p, c_f64p]),
     ("wmd_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("wmd_last_launch_count", ctypes.c_int, [ctypes.c_void_p]),
     ("wmd_query_topk", ctypes.c_int,

@@ -209,6 +209,8 @@ wmd_status finish(wmd_handle* h) {
   const unsigned bits = *h->err_host;
   if (bits) {
     clear_err(h);
+    if (bits & ERR_TIMEOUT)
+      return fail(WMD_ERR_DEVICE_TIMEOUT, "device error:" + describe_err_bits(bits));
     return fail(WMD_ERR_INVALID_INPUT, "invalid input:" + describe_err_bits(bits));
   }
   return WMD_OK;
@@ -1063,6 +1065,11 @@ wmd_status default_handle(wmd_handle** out) {
   if (!tl_handle.h) {
     wmd_status s = wmd_create(&tl_handle.h, dev);
     if (s) return s;
+    // The drop-in calls build their cost panel on the tensor cores in the
+    // FP32-accurate split-TF32 form (FP32 rows read in place, three TF32
+    // products); widths it cannot tile (d % 4 != 0) take the FP32 CUDA-core
+    // panel.  Both hold the plain path's 1e-5 against the reference.
+    tl_handle.h->mode = WMD_CDIST_TF32X3;
   }
   *out = tl_handle.h;
   return WMD_OK;
@@ -1153,6 +1160,7 @@ const char* wmd_status_string(wmd_status s) {
     case WMD_ERR_CUDA: return "CUDA error";
     case WMD_ERR_NO_DEVICE: return "no CUDA device";
     case WMD_ERR_UNSUPPORTED: return "unsupported";
+    case WMD_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
   }
   return "unknown status";
 }
@@ -1367,6 +1375,18 @@ wmd_status wmd_topk_device(wmd_handle* h, const double* scores_dev, uint64_t n,
   wmd_status s = bind(h);
   if (s) return s;
   return topk_device(h, scores_dev, n, k, idx_dev, val_dev);
+}
+
+wmd_status wmd_selftest_bounded_wait(wmd_handle* h, uint64_t limit_ns) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (limit_ns < 1000 || limit_ns > 2000000000ull)
+    return fail(WMD_ERR_INVALID_ARG, "limit_ns outside [1e3, 2e9]");
+  wmd_status s = bind(h);
+  if (s) return s;
+  h->last_launches = launch_wait_selftest(h->err_dev.as<unsigned>(), limit_ns, h->stream);
+  CK(cudaGetLastError());
+  set_last_error("");
+  return WMD_OK;
 }
 
 wmd_status wmd_check(wmd_handle* h) {

@@ -20,6 +20,9 @@
 // it names a host-side stand-in), so the first call on each device, with that
 // device current, looks the address up with cudaGetSymbolAddress and caches
 // it.  Make that first call before any stream capture begins on the device.
+// The cached address lives as long as the device's primary context: after
+// cudaDeviceReset on a device, this entry point must not be called on it
+// again in the same process.
 //
 // The kernels are the library's regular ones (norms, target packing and
 // validation, source selection, FP32 cost panel, near-pair fix-up, fused
@@ -85,6 +88,19 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
     return noalloc_fail(WMD_ERR_UNSUPPORTED, "vr_cap above 1024");
   if (V > 0xFFFFFFFFull || N >= 0x7FFFFFFFull)
     return noalloc_fail(WMD_ERR_UNSUPPORTED, "vocabulary or document count too large");
+  // Each factor of the scratch sizes below is bounded first, so that none of
+  // the size products can wrap around: anything larger cannot fit anyway.
+  if (d > kScratchBytes / 4 || nnz > kScratchBytes / 8 || N > kScratchBytes / 8) {
+    snprintf(msg, sizeof(msg),
+             "d, nnz or N too large for the fixed scratch of %zu bytes (64 MiB)",
+             kScratchBytes);
+    return noalloc_fail(WMD_ERR_INVALID_ARG, msg);
+  }
+  // The FP32 cost panel reads the embeddings with 16-byte vector loads when
+  // d % 4 == 0; a misaligned base would fault, so it is refused here.
+  if (d % 4 == 0 && (reinterpret_cast<uintptr_t>(vecs_dev) & 15u) != 0)
+    return noalloc_fail(WMD_ERR_INVALID_ARG,
+                        "vecs_dev must be 16-byte aligned when d % 4 == 0");
 
   // Carve the scratch: everything 256-byte aligned.
   const uint32_t cap = (uint32_t)vr_cap;
@@ -105,16 +121,22 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
   const unsigned near_cap = 4096;  // near-pair list (overflow -> panel scan)
   const size_t o_ncnt = off;   off += align256(sizeof(unsigned));
   const size_t o_npairs = off; off += align256((size_t)near_cap * 8);
+  const float expo = (float)(-lambda);
+  const bool want_km = expo == 0.f;  // K.*M is needed only for lambda = 0
   const size_t o_K = off;      off += align256((size_t)V * ld * 4);
-  const size_t o_KM = off;     off += align256((size_t)V * ld * 4);
+  const size_t o_KM = off;     off += want_km ? align256((size_t)V * ld * 4) : 0;
   if (off > kScratchBytes) {
     snprintf(msg, sizeof(msg),
              "problem needs %zu bytes of scratch; the fixed scratch holds %zu "
-             "bytes (64 MiB): 2*V*round4(vr_cap)*4 + V*4 + nnz*8 + ... too large",
+             "bytes (64 MiB): V*round4(vr_cap)*4 (twice for lambda = 0) + V*4 + "
+             "nnz*8 + ... too large",
              off, kScratchBytes);
     return noalloc_fail(WMD_ERR_INVALID_ARG, msg);
   }
 
+  // A pending error from earlier, unrelated work on this thread would
+  // otherwise be reported as this call's failure by the final check.
+  cudaGetLastError();
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
@@ -138,7 +160,7 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
   int64_t* cp = reinterpret_cast<int64_t*>(base + o_cp);
   uint2* ent = reinterpret_cast<uint2*>(base + o_ent);
   float* K = reinterpret_cast<float*>(base + o_K);
-  float* KM = reinterpret_cast<float*>(base + o_KM);
+  float* KMp = want_km ? reinterpret_cast<float*>(base + o_KM) : nullptr;
 
   NearList near;
   near.pairs = reinterpret_cast<uint2*>(base + o_npairs);
@@ -159,8 +181,6 @@ extern "C" wmd_status wmd_sinkhorn_noalloc(
   launch_pack_targets(col_ptr_dev, row_inds_dev, vals_dev, V, N, nnz, cp, ent,
                       err, st);
   launch_select(r_dev, V, vecs_dev, nE, d, sel, err, st);
-  const float expo = (float)(-lambda);
-  float* KMp = expo == 0.f ? KM : nullptr;  // K.*M is needed only for lambda = 0
   launch_cdist_fp32(vecs_dev, nE, V, d, sel, expo, K, KMp, ld, near, st);
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

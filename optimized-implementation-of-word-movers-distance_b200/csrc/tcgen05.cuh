@@ -36,12 +36,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
                : "memory");
 }
 // Waits for the phase of parity `par` to complete.  Bounded: returns false
-// (and flags the error word) after kWaitNs of wall-clock time.  Each try_wait
-// carries a suspend-time hint, so a waiting thread sleeps in hardware until
-// the phase completes instead of spinning on issue slots that the MMA-issuing
-// and converting warps of the same SM sub-partition need.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par,
-                                          unsigned* err) {
+// (and flags the error word) after limit_ns of wall-clock time.  Each
+// try_wait carries a suspend-time hint, so a waiting thread sleeps in
+// hardware until the phase completes instead of spinning on issue slots that
+// the MMA-issuing and converting warps of the same SM sub-partition need.
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t par,
+                                             unsigned* err,
+                                             unsigned long long limit_ns) {
   const uint32_t a = smem_u32(bar);
   unsigned long long t0 = 0;
   for (uint32_t i = 0;; ++i) {
@@ -57,12 +58,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par,
     if ((i & 63) == 0) {
       const unsigned long long t = gtime();
       if (t0 == 0) t0 = t;
-      else if (t - t0 > kWaitNs) {
+      else if (t - t0 > limit_ns) {
         atomicOr(err, ERR_TIMEOUT);
         return false;
       }
     }
   }
+}
+// The kernels' wait: bounded by kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par,
+                                          unsigned* err) {
+  return mbar_wait_ns(bar, par, err, kWaitNs);
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm,
                                             uint64_t* bar, int x, int y) {

@@ -347,6 +347,10 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
                    float* u0, int64_t ldu, unsigned* err, int num_sms,
                    cudaStream_t st);
 
+// Self-test of the bounded device-side wait (selftest.cu): a wait that can
+// only end through its limit; sets ERR_TIMEOUT in *err.
+int launch_wait_selftest(unsigned* err, unsigned long long limit_ns, cudaStream_t st);
+
 // GPU CSC build from an edge list (csc_build.cu).  The result equals the
 // host's stable counting sorts word-major (file order within a word,
 // sinkhorn_wmd_fused.cpp:493-506) then document-major: entries sorted by

@@ -1,7 +1,7 @@
 """Generate tests/golden/golden.json from the reference itself.
 
-    make -C oracle            # builds oracle/_ref/ from the reference sources
-    python tests/golden/make_golden.py
+    WMD_REFERENCE_DIR=<reference checkout> make -C oracle   # builds oracle/_ref/
+    WMD_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
 
 Needs the reference checkout (its data/ directory and its sources, compiled
 in place into oracle/_ref/).  Records, at full FP64 precision:
@@ -25,7 +25,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("WMD_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("WMD_REFERENCE_DIR", "")
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("set WMD_REFERENCE_DIR to the reference checkout "
+                     "(the directory holding sinkhorn_wmd_fused.cpp)")
 sys.path.insert(0, REPO)
 sys.path.insert(0, HERE)
 
