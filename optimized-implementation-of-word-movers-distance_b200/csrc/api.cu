@@ -95,13 +95,13 @@ struct QueryKey {
   float tol = 0.f;
   float omega = 1.f;
   int prec = -1;
-  const void* bufs[17] = {};  // every device buffer the graph reads or writes
+  const void* bufs[18] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
           epoch == o.epoch && tol == o.tol && omega == o.omega && prec == o.prec))
       return false;
-    for (int i = 0; i < 17; ++i)
+    for (int i = 0; i < 18; ++i)
       if (bufs[i] != o.bufs[i]) return false;
     return true;
   }
@@ -143,6 +143,11 @@ struct wmd_handle {
   DevBuf r_dev, sel_ids, sel_rinv, sel_S, sel_nS, sel_S16, sel_vr, sel_chunks,
       K, KM, K16, out_dev, err_dev, near_pairs, near_count, iters;
   DevBuf vstate;  // each target word's previous v (over-relaxed solves)
+  // Row-scaled panels (panel_rescale.cu): row minima of M per query, and the
+  // largest squared embedding norm, which decides when they are needed.
+  DevBuf mrow, emax_dev;
+  float emax2 = 0.f;
+  DevBuf exact_list, exact_count;  // documents re-solved in FP64 (exact_f64.cu)
   // batched queries
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
   // Second pipeline slot of the batched queries (its own stream and
@@ -150,7 +155,7 @@ struct wmd_handle {
   // one source's solve tail overlaps the next source's cost panel and solve.
   struct BatchSlot {
     DevBuf sel_S, sel_nS, sel_S16, near_pairs, near_count, K, KM, K16, vstate,
-        ws_Asrc, ws_u0;
+        ws_Asrc, ws_u0, mrow, exact_list, exact_count;
   } slot1;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t join[2] = {nullptr, nullptr};
@@ -216,6 +221,31 @@ wmd_status finish(wmd_handle* h) {
   return WMD_OK;
 }
 
+uint32_t max_doc_len(const wmd_handle* h) {
+  uint32_t m = 0;
+  for (uint32_t l : h->doc_len) m = std::max(m, l);
+  return m;
+}
+
+// Largest squared row norm of the embeddings now on the device (synchronises
+// the handle's stream once; embeddings are set far less often than queried).
+wmd_status update_emax(wmd_handle* h, uint64_t V) {
+  CK(h->emax_dev.ensure(sizeof(unsigned)));
+  launch_max_norm(h->nE.as<float>(), V, h->emax_dev.as<unsigned>(), h->stream);
+  unsigned bits = 0;
+  CK(cudaMemcpyAsync(&bits, h->emax_dev.p, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  memcpy(&h->emax2, &bits, sizeof(float));
+  return WMD_OK;
+}
+
+// Whether a query with this exponent needs the row-scaled panel: lambda * M
+// can exceed kScaleLimit (M <= 2 max |E_w|; FP32 exp underflows near 87).
+bool row_scaled(const wmd_handle* h, float expo) {
+  return expo != 0.f && -expo * 2.f * sqrtf(h->emax2) > kScaleLimit;
+}
+
 wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
                           uint64_t d, int where, bool f64) {
   if (!h || !vecs || V == 0 || d == 0 || (where != 0 && where != 1))
@@ -247,6 +277,9 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
     launches += launch_embed_norms(h->E32.as<float>(), V, d, h->nE.as<float>(),
                                    h->stream);
   }
+  s = update_emax(h, V);
+  if (s) return s;
+  launches += 1;
   CK(cudaGetLastError());
   h->V = V;
   h->d = d;
@@ -536,6 +569,15 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   near.E32 = h->E32.as<float>();
   near.S32 = sel.S;
   near.d = (int)d;
+  // Row-scaled panel when lambda * M can underflow FP32 (panel_rescale.cu).
+  float* mrow = nullptr;
+  const int mdl = (int)max_doc_len(h);
+  if (row_scaled(h, expo)) {
+    CK(h->mrow.ensure((size_t)V * sizeof(float)));
+    CK(h->exact_list.ensure(exact_f64_list_cap() * sizeof(int32_t)));
+    CK(h->exact_count.ensure(sizeof(unsigned)));
+    mrow = h->mrow.as<float>();
+  }
   // Learned warm start (needs lambda != 0: its features read M = ln K / expo).
   const bool ws = h->ws_on && h->ws_d == (int)d && expo != 0.f;
   if (ws) {
@@ -560,23 +602,29 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
                        tcm ? h->E16.p : nullptr, tcm ? h->sel_S16.p : nullptr, dp,
                        near.count);  // the selection also zeroes the near-pair count
     CK(record(1, capturing));
+    if (mrow) CK(cudaMemsetAsync(mrow, 0x7f, (size_t)V * sizeof(float), h->stream));
     if (tcm || x3) {
       const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
                                      h->E16.p, h->sel_S16.p,
                                      h->E32.as<float>(), h->nE.as<float>(), V, d,
                                      sel, expo, h->K.as<float>(), KMp, ld, near,
-                                     h->err_dev.as<unsigned>(), h->sms, h->stream);
+                                     h->err_dev.as<unsigned>(), h->sms, h->stream, mrow);
       if (lc < 0)
         return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable "
                                          "(tensor map encoding failed)");
       n += lc;
     } else {
       n += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d, sel,
-                             expo, h->K.as<float>(), KMp, ld, near, h->stream);
+                             expo, h->K.as<float>(), KMp, ld, near, h->stream, mrow);
     }
     n += launch_near_fixup(near, expo, h->K.as<float>(), KMp, ld, V,
-                           h->nE.as<float>(), sel.nS, sel.vr, h->sms, h->stream);
+                           h->nE.as<float>(), sel.nS, sel.vr, h->sms, h->stream,
+                           mrow != nullptr);
+    if (mrow)
+      n += launch_panel_rescale(h->K.as<float>(), ld, V, sel.vr, mrow, expo, h->sms,
+                                h->stream);
     SolveCtl ctl;
+    ctl.mrow = mrow;
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->iters.as<int>();
@@ -587,7 +635,7 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
                           h->ws_params.as<float>(), sel.S, sel.rinv, (int)cap,
                           h->K.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
                           h->ws_Asrc.as<float>(), h->ws_u0.as<float>(), ld,
-                          h->err_dev.as<unsigned>(), h->sms, h->stream);
+                          h->err_dev.as<unsigned>(), h->sms, h->stream, mrow);
       ctl.u0 = h->ws_u0.as<float>();
       ctl.ldu = ld;
     }
@@ -604,6 +652,14 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     } else {
       n += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t, ctl,
                         out_dev, h->stream);
+    }
+    if (mrow) {  // documents the row-scaled FP32 panel cannot carry, in FP64
+      const int le = launch_exact_f64(h->E32.as<float>(), d, sel, t, expo, ctl, mdl,
+                                      h->exact_list.as<int32_t>(),
+                                      h->exact_count.as<unsigned>(), h->sms, out_dev,
+                                      h->stream);
+      if (le < 0) return fail(WMD_ERR_UNSUPPORTED, "documents too long for the FP64 re-solve");
+      n += le;
     }
     CK(record(3, capturing));
     CK(cudaGetLastError());
@@ -627,11 +683,11 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.omega = h->omega;
   key.prec = (int)h->prec + (ws ? 2 : 0);
   {
-    const DevBuf* used[17] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+    const DevBuf* used[18] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
                               &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
                               &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16,
-                              &h->ws_Asrc, &h->ws_u0, &h->vstate};
-    for (int i = 0; i < 17; ++i) key.bufs[i] = used[i]->p;
+                              &h->ws_Asrc, &h->ws_u0, &h->vstate, &h->mrow};
+    for (int i = 0; i < 18; ++i) key.bufs[i] = used[i]->p;
   }
   if (!h->use_graphs) {
     int n = 0;
@@ -799,6 +855,13 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   if (h->prec == WMD_SOLVE_BF16 && !need_km)
     for (uint64_t s = 0; s < S; ++s) ld16_max = std::max(ld16_max, block_panel_width(vrs[s]));
   if (ld16_max) CK(h->K16.ensure((size_t)V * ld16_max * 2));
+  const bool scaled = row_scaled(h, expo);  // panel_rescale.cu
+  const int mdl = (int)max_doc_len(h);
+  if (scaled) {
+    CK(h->mrow.ensure((size_t)V * sizeof(float)));
+    CK(h->exact_list.ensure(exact_f64_list_cap() * sizeof(int32_t)));
+    CK(h->exact_count.ensure(sizeof(unsigned)));
+  }
   const bool ws = h->ws_on && h->ws_d == (int)d && expo != 0.f;
   if (ws) {
     wmd_status sw = ws_prepare_docs(h);
@@ -830,6 +893,11 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     }
     CK(b1.near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
     CK(b1.near_count.ensure(sizeof(unsigned)));
+    if (scaled) {
+      CK(b1.mrow.ensure((size_t)V * sizeof(float)));
+      CK(b1.exact_list.ensure(exact_f64_list_cap() * sizeof(int32_t)));
+      CK(b1.exact_count.ensure(sizeof(unsigned)));
+    }
     if (tcm) CK(b1.sel_S16.ensure((size_t)vr_max * dp * 2));
   }
   int launches = 0;
@@ -880,6 +948,7 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     DevBuf& bAs = in1 ? h->slot1.ws_Asrc : h->ws_Asrc;
     DevBuf& bU0 = in1 ? h->slot1.ws_u0 : h->ws_u0;
     float* KMs = need_km ? (in1 ? h->slot1.KM : h->KM).as<float>() : nullptr;
+    float* mrow = scaled ? (in1 ? h->slot1.mrow : h->mrow).as<float>() : nullptr;
     SourceSel sel;
     sel.ids = h->b_ids.as<uint32_t>() + off;
     sel.rinv = h->b_rinv.as<float>() + off;
@@ -899,12 +968,13 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                                       tcm ? h->E16.p : nullptr,
                                       tcm ? bS16.p : nullptr, dp, sst);
     CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), sst));
+    if (mrow) CK(cudaMemsetAsync(mrow, 0x7f, (size_t)V * sizeof(float), sst));
     if (tcm || x3) {
       const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
                                      h->E16.p, bS16.p, h->E32.as<float>(),
                                      h->nE.as<float>(), V, d, sel, expo,
                                      bK.as<float>(), KMs, ld, near,
-                                     h->err_dev.as<unsigned>(), h->sms, sst);
+                                     h->err_dev.as<unsigned>(), h->sms, sst, mrow);
       if (lc < 0) {
         if (overlap) cudaStreamSynchronize(h->stream2);
         return fail(WMD_ERR_UNSUPPORTED, "tensor-core cost panel unavailable");
@@ -912,11 +982,16 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
       launches += lc;
     } else {
       launches += launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d,
-                                    sel, expo, bK.as<float>(), KMs, ld, near, sst);
+                                    sel, expo, bK.as<float>(), KMs, ld, near, sst, mrow);
     }
     launches += launch_near_fixup(near, expo, bK.as<float>(), KMs, ld, V,
-                                  h->nE.as<float>(), sel.nS, sel.vr, h->sms, sst);
+                                  h->nE.as<float>(), sel.nS, sel.vr, h->sms, sst,
+                                  mrow != nullptr);
+    if (mrow)
+      launches += launch_panel_rescale(bK.as<float>(), ld, V, sel.vr, mrow, expo,
+                                       h->sms, sst);
     SolveCtl ctl;
+    ctl.mrow = mrow;
     ctl.max_iter = max_iter;
     ctl.tol = h->tol;
     ctl.iters = h->b_iters.as<int>() + s * N;
@@ -927,7 +1002,7 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                                  h->ws_params.as<float>(), sel.S, sel.rinv, (int)vr,
                                  bK.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
                                  bAs.as<float>(), bU0.as<float>(), ld,
-                                 h->err_dev.as<unsigned>(), h->sms, sst);
+                                 h->err_dev.as<unsigned>(), h->sms, sst, mrow);
       ctl.u0 = bU0.as<float>();
       ctl.ldu = ld;
     }
@@ -955,6 +1030,18 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
       return fail(WMD_ERR_UNSUPPORTED, "a source has more than 1024 words");
     }
     launches += ls;
+    if (mrow) {  // documents the row-scaled FP32 panel cannot carry, in FP64
+      DevBuf& bL = in1 ? h->slot1.exact_list : h->exact_list;
+      DevBuf& bC = in1 ? h->slot1.exact_count : h->exact_count;
+      const int le = launch_exact_f64(h->E32.as<float>(), d, sel, t, expo, ctl, mdl,
+                                      bL.as<int32_t>(), bC.as<unsigned>(), h->sms,
+                                      h->b_out.as<double>() + s * N, sst);
+      if (le < 0) {
+        if (overlap) cudaStreamSynchronize(h->stream2);
+        return fail(WMD_ERR_UNSUPPORTED, "documents too long for the FP64 re-solve");
+      }
+      launches += le;
+    }
   }
   if (overlap) {  // the results wait for both slots
     CK(cudaEventRecord(h->join[1], h->stream2));
@@ -1035,6 +1122,9 @@ wmd_status set_embeddings_needed(wmd_handle* h, const double* vecs_mapped,
       h->need.as<unsigned char>(), h->E32.as<float>(), h->nE.as<float>(),
       h->need_count.as<unsigned long long>(), h->stream);
   CK(cudaGetLastError());
+  wmd_status se = update_emax(h, V);
+  if (se) return se;
+  launches += 1;
   h->V = V;
   h->d = d;
   h->have_E = true;
@@ -1612,10 +1702,21 @@ wmd_status wmd_ws_build_training_set(wmd_handle* h, const uint64_t* src_ptr,
     launch_gather_sources(sel_s.ids, (int)vr, h->E32.as<float>(), h->nE.as<float>(), d,
                           sel_s.S, sel_s.nS, nullptr, nullptr, 0, h->stream);
     CK(cudaMemsetAsync(near.count, 0, sizeof(unsigned), h->stream));
+    // row-scaled panel when lambda * M can underflow FP32 (panel_rescale.cu);
+    // the labels u are the same either way
+    float* mrow = nullptr;
+    if (row_scaled(h, expo)) {
+      CK(h->mrow.ensure((size_t)V * sizeof(float)));
+      mrow = h->mrow.as<float>();
+      CK(cudaMemsetAsync(mrow, 0x7f, (size_t)V * sizeof(float), h->stream));
+    }
     launch_cdist_fp32(h->E32.as<float>(), h->nE.as<float>(), V, d, sel_s, expo,
-                      h->K.as<float>(), nullptr, ld, near, h->stream);
+                      h->K.as<float>(), nullptr, ld, near, h->stream, mrow);
     launch_near_fixup(near, expo, h->K.as<float>(), nullptr, ld, V, h->nE.as<float>(),
-                      sel_s.nS, sel_s.vr, h->sms, h->stream);
+                      sel_s.nS, sel_s.vr, h->sms, h->stream, mrow != nullptr);
+    if (mrow)
+      launch_panel_rescale(h->K.as<float>(), ld, V, sel_s.vr, mrow, expo, h->sms,
+                           h->stream);
     // documents of this source: a seeded sample without replacement
     for (uint32_t q = 0; q < D; ++q) {
       const uint64_t k = q + rng() % (nonempty.size() - q);
@@ -1655,7 +1756,7 @@ wmd_status wmd_ws_build_training_set(wmd_handle* h, const uint64_t* src_ptr,
                    expo, ids_d.as<uint32_t>(), r64_d.as<double>(), (int)vr, t.col_ptr,
                    t.ent, docs_d.as<int32_t>(), u_d.as<double>(), (int)D,
                    sel_d.as<int32_t>(), G, row0_d.as<int64_t>(), L.F,
-                   h->ws_X.as<float>(), h->ws_y.as<float>(), h->stream);
+                   h->ws_X.as<float>(), h->ws_y.as<float>(), h->stream, mrow);
     CK(cudaStreamSynchronize(h->stream));  // host vectors reused next source
     CK(cudaGetLastError());
   }

@@ -15,6 +15,11 @@
 // formula (fused:35-43), in FP32.
 // Padding columns i >= v_r are written as K = KM = 0.  KM is written only when
 // the caller passes a buffer for it (the solve needs it only for expo = 0).
+//
+// Row-scaled form (mrow given, expo != 0): the panel receives M itself and
+// mrow[w] the smallest M of row w (atomicMin on the float bits, M >= 0);
+// panel_rescale_kernel then turns M into K' = exp(expo (M - mrow[w])) once
+// the near pairs are fixed.  See panel_rescale.cu for why.
 #include "wmd_internal.cuh"
 
 namespace wmd {
@@ -48,7 +53,7 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
                   const float* __restrict__ nS,
                   const uint32_t* __restrict__ vr_dev, float expo,
                   float* __restrict__ Kout, float* __restrict__ KMout, int ld,
-                  const NearList near) {
+                  const NearList near, float* __restrict__ mrow) {
   __shared__ __align__(16) float As[2][BK][AS];
   __shared__ __align__(16) float Bs[2][BK][BN];
   const int tid = threadIdx.x;
@@ -175,6 +180,7 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
     if (w >= V) break;
     const float ne = active ? nE[w] : 0.f;
     float kv[4], kmv[4];
+    float mmin = __int_as_float(0x7f7f7f7f);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       kv[j] = 0.f;
@@ -185,14 +191,20 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
         const float m2 = fmaxf(ne + ns - 2.f * acc[i][j], 0.f);
         if (m2 < near_threshold(ne, ns)) near_pair(near, w, c);
         const float m = sqrtf(m2);
-        const float k = expf(expo * m);
-        kv[j] = k;
-        kmv[j] = k * m;
+        if (mrow) {  // row-scaled form: M now, K' after the fix-up
+          kv[j] = m;
+          mmin = fminf(mmin, m);
+        } else {
+          const float k = expf(expo * m);
+          kv[j] = k;
+          kmv[j] = k * m;
+        }
       }
     }
+    if (mrow && c0 < vr) atomicMin(reinterpret_cast<int*>(mrow + w), __float_as_int(mmin));
     *reinterpret_cast<float4*>(Kout + w * (uint64_t)ld + c0) =
         make_float4(kv[0], kv[1], kv[2], kv[3]);
-    if (KMout)
+    if (KMout && !mrow)
       *reinterpret_cast<float4*>(KMout + w * (uint64_t)ld + c0) =
           make_float4(kmv[0], kmv[1], kmv[2], kmv[3]);
   }
@@ -200,14 +212,14 @@ cdist_fp32_kernel(const float* __restrict__ E, const float* __restrict__ nE,
 
 int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
                       const SourceSel& s, float expo, float* K, float* KM,
-                      int ld, const NearList& near, cudaStream_t st) {
+                      int ld, const NearList& near, cudaStream_t st, float* mrow) {
   dim3 grid((unsigned)((V + BM - 1) / BM), (unsigned)((ld + BN - 1) / BN));
   if (d % 4 == 0)
     cdist_fp32_kernel<true><<<grid, THREADS, 0, st>>>(E32, nE, V, (int)d, s.S, s.nS,
-                                                      s.vr, expo, K, KM, ld, near);
+                                                      s.vr, expo, K, KM, ld, near, mrow);
   else
     cdist_fp32_kernel<false><<<grid, THREADS, 0, st>>>(E32, nE, V, (int)d, s.S, s.nS,
-                                                       s.vr, expo, K, KM, ld, near);
+                                                       s.vr, expo, K, KM, ld, near, mrow);
   return 1;
 }
 

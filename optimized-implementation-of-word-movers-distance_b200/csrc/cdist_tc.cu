@@ -87,6 +87,7 @@ struct Params {
   float* K;           // [V][ld]
   float* KM;          // [V][ld] or null (then K*M is not stored)
   NearList near;      // cancellation-prone pairs for the exact fix-up pass
+  float* mrow;        // row-scaled form: [V] row minima of M (else null)
   unsigned* err;
   uint64_t V;
   int d, ld, NT, KT, tmem_cols, stages;
@@ -348,6 +349,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
         const uint64_t w = (uint64_t)tile * BM + row;
         const bool wok = w < p.V;
         const float ne = wok ? p.nE[w] : 0.f;  // issued before the wait
+        float mmin = __int_as_float(0x7f7f7f7f);  // row-scaled form
         if (!mbar_wait(&accf[b], tph, p.err)) break;
         fence_after();
         for (int c0 = 16 * half; c0 < p.NT; c0 += 32) {
@@ -367,17 +369,32 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
           // columns past v_r are zeroed last.
           float kv[16], kmv[16];
           unsigned nearmask = 0;
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const float ns = nS_s[c0 + j];
-            const float m2 = fmaxf(ne + ns - 2.f * acc[j], 0.f);
-            nearmask |= (m2 < near_threshold(ne, ns) ? 1u : 0u) << j;
-            const float m = sqrtf(m2);
-            const float kx = expf(p.expo * m);
-            kv[j] = kx;
-            kmv[j] = kx * m;
-          }
           const int nval = vr - (n0 + c0);  // valid columns of this chunk
+          if (p.mrow) {
+            // Row-scaled form: M now (and the row minimum), K' after the
+            // near-pair fix-up (panel_rescale.cu).
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const float ns = nS_s[c0 + j];
+              const float m2 = fmaxf(ne + ns - 2.f * acc[j], 0.f);
+              nearmask |= (m2 < near_threshold(ne, ns) ? 1u : 0u) << j;
+              const float m = sqrtf(m2);
+              kv[j] = m;
+              kmv[j] = 0.f;
+              if (j < nval) mmin = fminf(mmin, m);
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const float ns = nS_s[c0 + j];
+              const float m2 = fmaxf(ne + ns - 2.f * acc[j], 0.f);
+              nearmask |= (m2 < near_threshold(ne, ns) ? 1u : 0u) << j;
+              const float m = sqrtf(m2);
+              const float kx = expf(p.expo * m);
+              kv[j] = kx;
+              kmv[j] = kx * m;
+            }
+          }
           if (nval < 16) {
 #pragma unroll
             for (int j = 0; j < 16; ++j)
@@ -400,12 +417,14 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             if (c < p.ld) {
               *reinterpret_cast<float4*>(krow + c) = make_float4(
                   kv[4 * j4], kv[4 * j4 + 1], kv[4 * j4 + 2], kv[4 * j4 + 3]);
-              if (p.KM)
+              if (p.KM && !p.mrow)
                 *reinterpret_cast<float4*>(kmrow + c) = make_float4(
                     kmv[4 * j4], kmv[4 * j4 + 1], kmv[4 * j4 + 2], kmv[4 * j4 + 3]);
             }
           }
         }
+        if (p.mrow && wok && mmin < __int_as_float(0x7f7f7f7f))
+          atomicMin(reinterpret_cast<int*>(p.mrow + w), __float_as_int(mmin));
         fence_before();
         mbar_arrive(&acce[b]);
       }
@@ -552,7 +571,7 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
                     const NearList& near, unsigned* err, int num_sms,
-                    cudaStream_t st) {
+                    cudaStream_t st, float* mrow) {
   const bool x3 = form == TC_TF32X3;
   const uint64_t rows_b = s.cap ? s.cap : 1;
   int NT, KT;
@@ -590,6 +609,7 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
   p.K = K;
   p.KM = KM;
   p.near = near;
+  p.mrow = mrow;
   p.err = err;
   p.V = V;
   p.d = (int)d;

@@ -8,6 +8,10 @@
 // sinkhorn_wmd_fused.cpp:35-43 — one warp per pair with the lanes splitting the
 // d coordinates, and rewrites K (and K.*M when stored).
 //
+// In the row-scaled form (scaled = true) the panel still holds M at this
+// point: the exact M is written instead of K, and panel_rescale_kernel turns
+// every entry into K' afterwards.
+//
 // Near pairs are few (a source word against itself, true near-duplicates), so
 // the list is normally short.  If more pairs turned up than the list holds,
 // the kernel falls back to scanning the whole panel for near entries (M is
@@ -20,7 +24,7 @@ __global__ void near_fixup_kernel(NearList nl, float expo, float* __restrict__ K
                                   float* __restrict__ KM, int ld, uint64_t V,
                                   const float* __restrict__ nE,
                                   const float* __restrict__ nS,
-                                  const uint32_t* __restrict__ vr_dev) {
+                                  const uint32_t* __restrict__ vr_dev, bool scaled) {
   const int lane = threadIdx.x & 31;
   const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -31,9 +35,13 @@ __global__ void near_fixup_kernel(NearList nl, float expo, float* __restrict__ K
                                  nl.S32 + (uint64_t)i * nl.d, nl.d, lane);
     if (lane == 0) {
       const float m = sqrtf(m2);
-      const float k = expf(expo * m);
-      K[w * (uint64_t)ld + i] = k;
-      if (KM) KM[w * (uint64_t)ld + i] = k * m;
+      if (scaled) {
+        K[w * (uint64_t)ld + i] = m;
+      } else {
+        const float k = expf(expo * m);
+        K[w * (uint64_t)ld + i] = k;
+        if (KM) KM[w * (uint64_t)ld + i] = k * m;
+      }
     }
   };
   for (uint64_t p = gw; p < listed; p += nw) {
@@ -50,7 +58,7 @@ __global__ void near_fixup_kernel(NearList nl, float expo, float* __restrict__ K
       bool near = false;
       if (i < vr) {
         const float kv = K[w * (uint64_t)ld + i];
-        const float m = expo != 0.f ? logf(kv) / expo : KM[w * (uint64_t)ld + i];
+        const float m = scaled ? kv : expo != 0.f ? logf(kv) / expo : KM[w * (uint64_t)ld + i];
         near = m * m < near_threshold(ne, nS[i]);
       }
       unsigned msk = __ballot_sync(0xffffffffu, near);
@@ -65,10 +73,10 @@ __global__ void near_fixup_kernel(NearList nl, float expo, float* __restrict__ K
 
 int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
                       int ld, uint64_t V, const float* nE, const float* nS,
-                      const uint32_t* vr, int num_sms, cudaStream_t st) {
+                      const uint32_t* vr, int num_sms, cudaStream_t st, bool scaled) {
   const int threads = 256;
   near_fixup_kernel<<<num_sms > 0 ? num_sms : 148, threads, 0, st>>>(
-      near, expo, K, KM, ld, V, nE, nS, vr);
+      near, expo, K, KM, ld, V, nE, nS, vr, scaled);
   return 1;
 }
 

@@ -71,6 +71,12 @@ namespace wmd {
 #ifndef WMD_SOLVE_DOT_CHAINS  // independent accumulators per dot product
 #define WMD_SOLVE_DOT_CHAINS 2
 #endif
+// Staged-row layout: 0 = 32-float row slices XOR-swizzled per lane (no
+// padding; every load computes its chunk address), 1 = slices padded to 36
+// floats (conflict-free at compile-time offsets, 12.5 % more shared memory).
+#ifndef WMD_SOLVE_PAD
+#define WMD_SOLVE_PAD 0
+#endif
 
 namespace {
 // Launch shape per lane layout: warps per CTA, CTAs per SM, staged rounds
@@ -106,6 +112,13 @@ __device__ __forceinline__ void zero_row(Row& r) {
 #pragma unroll
   for (int t = 0; t < 8; ++t) r.c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
+// Rows of padding words (past the end of a document) are all ones with
+// weight c = 0: then s = K_w . u > 0 for any u > 0 and v = c / s is exactly
+// 0, so they add nothing to x and need no test for c = 0.
+__device__ __forceinline__ void ones_row(Row& r) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) r.c[t] = make_float4(1.f, 1.f, 1.f, 1.f);
+}
 }  // namespace
 
 template <int LPW>
@@ -113,6 +126,9 @@ struct SolveShape {
   static constexpr int WPS = 32 / LPW;  // words per round
   static constexpr int RL = 32 * LPW;   // padded row length (floats)
   static constexpr int NCH = RL / 4;    // float4 chunks per padded row
+  // float4 slots per 32-float slice of a staged row (8 chunks, + 1 pad)
+  static constexpr int SLC = WMD_SOLVE_PAD ? 9 : 8;
+  static constexpr int SROW = LPW * SLC;  // float4 slots per staged row
   // Rounds of K rows kept in registers (fewer when the per-lane dimension
   // arrays of wide sources already use the register budget).
   static constexpr int RR = LPW <= 4 ? WMD_SOLVE_REG_ROUNDS : 1;
@@ -123,9 +139,11 @@ struct SolveShape {
   static __host__ __device__ size_t entries_bytes(int srounds) {
     return ((size_t)(srounds + RR) * WPS * 8 + 15) & ~(size_t)15;
   }
+  static __host__ __device__ size_t staged_bytes(int srounds) {
+    return (size_t)srounds * WPS * SROW * 16;
+  }
   static __host__ __device__ size_t warp_bytes(int srounds) {
-    return (size_t)srounds * WPS * RL * 4 + entries_bytes(srounds) +
-           32 * 32 * 4 + RL * 4;
+    return staged_bytes(srounds) + entries_bytes(srounds) + 32 * 32 * 4 + RL * 4;
   }
 };
 
@@ -139,7 +157,8 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              const int32_t* __restrict__ order, int64_t N, int max_iter,
              float tol, int* __restrict__ iters_out, int srounds,
              const float* __restrict__ u0, int64_t ldu, float omega,
-             float* __restrict__ vstate, double* __restrict__ out) {
+             float* __restrict__ vstate, const float* __restrict__ mrow,
+             double* __restrict__ out) {
   using Sh = SolveShape<LPW>;
   constexpr int WPS = Sh::WPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -148,8 +167,8 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   const int srows = srounds * WPS;
   unsigned char* wbase = smem_raw + (size_t)warp * Sh::warp_bytes(srounds);
   float4* sK = reinterpret_cast<float4*>(wbase);
-  uint2* sE = reinterpret_cast<uint2*>(wbase + (size_t)srows * Sh::RL * 4);
-  float* red = reinterpret_cast<float*>(wbase + (size_t)srows * Sh::RL * 4 +
+  uint2* sE = reinterpret_cast<uint2*>(wbase + Sh::staged_bytes(srounds));
+  float* red = reinterpret_cast<float*>(wbase + Sh::staged_bytes(srounds) +
                                         Sh::entries_bytes(srounds));
   float* ubuf = red + 32 * 32;
   const int vr = (int)*vr_dev;
@@ -220,33 +239,38 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     for (int k = lane; k < ne; k += 32)
       sE[k] = k < n ? __ldg(&ent[b + k]) : make_uint2(0u, 0u);
     __syncwarp();
-    // Register rows: rounds [0, rr); zero rows and weights elsewhere.
+    // Register rows: rounds [0, rr); padding rows (ones, c = 0) elsewhere.
+    // Chunks past the panel width stay zero (their u is 0).
     Row reg[RR];
     float creg[RR];
 #pragma unroll
     for (int t = 0; t < RR; ++t) {
-      zero_row(reg[t]);
       creg[t] = 0.f;
       const int k = t * WPS + g;
       if (t < rr && k < n) {
+        zero_row(reg[t]);
         const uint2 en = sE[k];
         creg[t] = __uint_as_float(en.y);
         const float4* rp = reinterpret_cast<const float4*>(K + (size_t)en.x * ld);
 #pragma unroll
         for (int c = 0; c < 8; ++c)
           if (8 * q + c < ldc) reg[t].c[c] = __ldg(rp + 8 * q + c);
+      } else {
+        ones_row(reg[t]);
       }
     }
-    // Staged rows: rounds [rr, rr + sr), padded with zero rows to whole rounds.
+    // Staged rows: rounds [rr, rr + sr), padded with ones rows to whole rounds.
     for (int c = lane; c < sr * WPS * Sh::NCH; c += 32) {
       const int s = c / Sh::NCH, lc = c % Sh::NCH;
       const int k = rr * WPS + s;
-      float4* dst = sK + (size_t)s * Sh::NCH + 8 * (lc >> 3) +
-                    ((lc & 7) ^ ((s * LPW + (lc >> 3)) & 7));
+      float4* dst = WMD_SOLVE_PAD
+                        ? sK + (size_t)(s * LPW + (lc >> 3)) * Sh::SLC + (lc & 7)
+                        : sK + (size_t)s * Sh::NCH + 8 * (lc >> 3) +
+                              ((lc & 7) ^ ((s * LPW + (lc >> 3)) & 7));
       if (k < n && lc < ldc)
         cp_async16(dst, K + (size_t)sE[k].x * ld + 4 * lc);
       else
-        *dst = make_float4(0.f, 0.f, 0.f, 0.f);
+        *dst = k < n ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(1.f, 1.f, 1.f, 1.f);
     }
     // Next document's pointers (the order[] load has landed by now).
     int64_t bn = 0;
@@ -261,21 +285,32 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     auto load_staged = [&](int s_round, Row& r, float& cval) {
       const int s = s_round * WPS + g;
       cval = __uint_as_float(sE[rr * WPS + s].y);
+#if WMD_SOLVE_PAD
+      const float4* rp = sK + (size_t)(s * LPW + q) * Sh::SLC;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) r.c[t] = rp[t];
+#else
       const float4* rp = sK + (size_t)s * Sh::NCH + 8 * q;
 #pragma unroll
       for (int t = 0; t < 8; ++t) r.c[t] = rp[t ^ key];
+#endif
     };
+    // A row from L2 (pad: the padding row for k >= n, else zeros).
     auto load_global = [&](const float* __restrict__ P, int k, Row& r,
-                           float& cval) {
-      zero_row(r);
+                           float& cval, bool pad) {
       cval = 0.f;
       if (k < n) {
+        zero_row(r);
         const uint2 en = __ldg(&ent[b + k]);
         cval = __uint_as_float(en.y);
         const float4* rp = reinterpret_cast<const float4*>(P + (size_t)en.x * ld);
 #pragma unroll
         for (int t = 0; t < 8; ++t)
           if (8 * q + t < ldc) r.c[t] = __ldg(rp + 8 * q + t);
+      } else if (pad) {
+        ones_row(r);
+      } else {
+        zero_row(r);
       }
     };
     auto dot = [&](const Row& r, const float2 (&u2)[16]) {
@@ -307,9 +342,17 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
         x2[2 * t + 1] = ffma2(make_float2(r.c[t].z, r.c[t].w), vv, x2[2 * t + 1]);
       }
     };
-    // v = c / s for a real word; exactly 0 for the padding words (c = 0 and
-    // a zero row), which would otherwise give 0/0.
-    auto weight = [](float c, float s) { return c != 0.f ? __fdividef(c, s) : 0.f; };
+    // The first word slot of a pass starts the accumulators (x = K_w v).
+    auto axpy_first = [&](const Row& r, float v, float2 (&x2)[16]) {
+      const float2 vv = make_float2(v, v);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        x2[2 * t] = __fmul2_rn(make_float2(r.c[t].x, r.c[t].y), vv);
+        x2[2 * t + 1] = __fmul2_rn(make_float2(r.c[t].z, r.c[t].w), vv);
+      }
+    };
+    // v = c / s; exactly 0 for the padding words (c = 0, s > 0).
+    auto weight = [](float c, float s) { return __fdividef(c, s); };
     // v of word k in a pass; over-relaxed (RLX) against the word's previous v
     // (vold, prefetched by vold_at with the word's row), which lane q = 0 of
     // the word's group keeps in vstate and broadcasts.
@@ -397,16 +440,15 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     // One pass of v = c ./ (K^T u), x += K v over all rounds of the document.
     auto pass = [&](const float2 (&u2)[16], float2 (&x2)[16]) {
       if constexpr (RLX) resv = 0.f;
-#pragma unroll
-      for (int t = 0; t < 16; ++t) x2[t] = make_float2(0.f, 0.f);
       {
         float sreg[RR], oreg[RR];
 #pragma unroll
         for (int t = 0; t < RR; ++t) oreg[t] = vold_at(t * WPS + g);
 #pragma unroll
         for (int t = 0; t < RR; ++t) sreg[t] = dot(reg[t], u2);
+        axpy_first(reg[0], vweight(creg[0], sreg[0], g, oreg[0]), x2);
 #pragma unroll
-        for (int t = 0; t < RR; ++t)
+        for (int t = 1; t < RR; ++t)
           axpy(reg[t], vweight(creg[t], sreg[t], t * WPS + g, oreg[t]), x2);
       }
       constexpr int U = SolveCfg<LPW>::kUnroll;
@@ -435,7 +477,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       for (int l = 0; l < lr; ++l) {
         Row ra;
         float ca;
-        load_global(K, (rr + sr + l) * WPS + g, ra, ca);
+        load_global(K, (rr + sr + l) * WPS + g, ra, ca, true);
         const float oa = vold_at((rr + sr + l) * WPS + g);
         axpy(ra, vweight(ca, dot(ra, u2), (rr + sr + l) * WPS + g, oa), x2);
       }
@@ -464,7 +506,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
         const bool ok = (dmask >> qq) & 1u;
         const float uo = ubuf[32 * qq + own];
         if (want_res && ok) res += fabsf(uo * tot[qq] - rw[qq]);
-        unew[qq] = ok ? relaxed_update(uo, __frcp_rn(rv[qq] * tot[qq]), RLX ? rg.omega : omega)
+        unew[qq] = ok ? relaxed_update(uo, __frcp_rn(rv[qq] * tot[qq]), RLX ? rg.omega : 1.f)
                       : 0.f;
       }
       if (want_res) {
@@ -487,7 +529,12 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
         uval[qq] = ((dmask >> qq) & 1u) ? __ldg(&u0[j * ldu + 32 * qq + own]) : 0.f;
       broadcast_u(uval, u2);
       const float rwm = step(uw, true);
-      const bool use_warm = isfinite(rwm) && !(rc < rwm);
+      // The warm candidate must also leave a finite u.
+      bool fin = true;
+#pragma unroll
+      for (int qq = 0; qq < LPW; ++qq) fin &= !((dmask >> qq) & 1u) || isfinite(uw[qq]);
+      fin = __all_sync(0xffffffffu, fin);
+      const bool use_warm = fin && isfinite(rwm) && !(rc < rwm);
 #pragma unroll
       for (int qq = 0; qq < LPW; ++qq) uval[qq] = use_warm ? uw[qq] : uc[qq];
       broadcast_u(uval, u2);
@@ -529,14 +576,14 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       } else if (t < rr + sr) {
         load_staged(t - rr, rk, ck);
       } else {
-        load_global(K, k, rk, ck);
+        load_global(K, k, rk, ck, true);
       }
       const float v = weight(ck, dot(rk, u2));
       float tk;
       if (FROM_KM) {
         Row rm;
         float cm;
-        load_global(KM, k, rm, cm);
+        load_global(KM, k, rm, cm, false);
         tk = dot(rm, u2);
       } else {
         // KM_i = K_i M_i = K_i log2(K_i) ln2 / expo; K_i = 0 contributes 0.
@@ -559,7 +606,13 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
           tk += __shfl_xor_sync(0xffffffffu, tk, off);
         tk *= km_scale;
       }
-      if (q == 0 && k < n) acc += (double)v * (double)tk;
+      if (q == 0 && k < n) {
+        acc += (double)v * (double)tk;
+        if (mrow) {  // row-scaled panel: + c_w m_w (panel_rescale.cu)
+          const uint32_t id = k < ne ? sE[k].x : __ldg(&ent[b + k]).x;
+          acc += (double)ck * (double)__ldg(&mrow[id]);
+        }
+      }
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -598,7 +651,7 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   if (sms_cache[dev] == 0) {
     const size_t per_warp = (kSmemPerSm / kBlocksPerSm - 1024) / kWarps;
     const size_t fixed = Sh::warp_bytes(0);
-    const size_t per_round = (size_t)Sh::WPS * (Sh::RL * 4 + 4);
+    const size_t per_round = Sh::staged_bytes(1) + (size_t)Sh::WPS * 8;
     int sr = per_warp > fixed ? (int)((per_warp - fixed) / per_round) : 0;
     while (sr > 0 && Sh::warp_bytes(sr) > per_warp) --sr;
     cudaFuncSetAttribute(solve_kernel<LPW, FROM_KM, RLX>,
@@ -617,7 +670,8 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   if (grid < 1) grid = 1;
   solve_kernel<LPW, FROM_KM, RLX><<<(unsigned)grid, kWarps * 32, smem, st>>>(
       K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
-      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, ctl.vstate, out);
+      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, ctl.vstate,
+      ctl.mrow, out);
   return 1;
 }
 

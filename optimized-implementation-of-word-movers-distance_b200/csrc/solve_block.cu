@@ -98,7 +98,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                    float tol, int* __restrict__ iters_out,
                    const float* __restrict__ u0, int64_t ldu, int max_rows,
                    float omega, float* __restrict__ vstate,
-                   double* __restrict__ out) {
+                   const float* __restrict__ mrow, double* __restrict__ out) {
   using Sh = BlockShape<NQ, kBW>;
   constexpr int kBT = kBW * 32;
   constexpr int RL = Sh::RL;
@@ -314,8 +314,12 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       const float rc = pass(ubufA, ubufA, true);
       const float rwm = pass(ubufB, ubufB, true);
       // Keep u0 unless its first-update residual is worse than the cold
-      // start's or not finite.
-      const bool use_warm = isfinite(rwm) && !(rc < rwm);
+      // start's or not finite, or its update is not finite (a prediction far
+      // off the cold start's scale can underflow v = c / (K^T u0) to 0).
+      bool fin = true;
+      for (int D = tid; D < vr; D += kBT) fin &= (bool)isfinite(ubufB[D]);
+      fin = __syncthreads_and(fin) != 0;
+      const bool use_warm = fin && isfinite(rwm) && !(rc < rwm);
       cur = use_warm ? ubufB : ubufA;
       res = use_warm ? rwm : rc;
       it = 1;
@@ -361,7 +365,12 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       const float s = pair_sum(dot(qa, u), dot(qb, u));
       const float v = weight(lo ? ca : cb, s);
       const float tk = pair_sum(kmdot(qa), kmdot(qb)) * km_scale;
-      if (lane == 0 || (lane == 16 && k + 1 < r1)) acc += (double)v * (double)tk;
+      if (lane == 0 || (lane == 16 && k + 1 < r1)) {
+        acc += (double)v * (double)tk;
+        if (mrow)  // row-scaled panel: + c_w m_w (panel_rescale.cu)
+          acc += (double)(lo ? ca : cb) *
+                 (double)__ldg(&mrow[__ldg(&ent[b + k + (lo ? 0 : 1)]).x]);
+      }
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -446,7 +455,7 @@ static int launch_block_t(const void* K16, int ld16, float expo,
   solve_block_kernel<NQ, kBW, kCPS, RLX><<<(unsigned)grid, kBW * 32, Sh::bytes(rows), st>>>(
       static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr,
       t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows, ctl.omega,
-      ctl.vstate, out);
+      ctl.vstate, ctl.mrow, out);
   return 1;
 }
 

@@ -105,7 +105,7 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                 const int32_t* __restrict__ order, int64_t N, int max_iter, float tol,
                 int* __restrict__ iters_out, const float* __restrict__ u0, int64_t ldu,
                 int cap, float omega, float* __restrict__ vstate,
-                double* __restrict__ out) {
+                const float* __restrict__ mrow, double* __restrict__ out) {
   using Sh = TcShape<NQ>;
   constexpr int RL = Sh::RL, RP = Sh::RP, KT = Sh::KT, DPW = Sh::DPW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -315,7 +315,13 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     if (warm) {
       const float rc = pass(ubufA, ubufA, true);
       const float rwm = pass(ubufB, ubufB, true);
-      const bool use_warm = isfinite(rwm) && !(rc < rwm);
+      // Keep u0 unless its first-update residual is worse than the cold
+      // start's or not finite, or its update is not finite (a prediction far
+      // off the cold start's scale can underflow v = c / (K^T u0) to 0).
+      bool fin = true;
+      for (int D = tid; D < vr; D += kTT) fin &= (bool)isfinite(ubufB[D]);
+      fin = __syncthreads_and(fin) != 0;
+      const bool use_warm = fin && isfinite(rwm) && !(rc < rwm);
       cur = use_warm ? ubufB : ubufA;
       res = use_warm ? rwm : rc;
       it = 1;
@@ -364,7 +370,11 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       float tk = a.x + a.y;
 #pragma unroll
       for (int off = 16; off; off >>= 1) tk += __shfl_xor_sync(0xffffffffu, tk, off);
-      if (lane == 0) acc += (double)sS[k] * (double)(tk * km_scale);
+      if (lane == 0) {
+        acc += (double)sS[k] * (double)(tk * km_scale);
+        if (mrow)  // row-scaled panel: + c_w m_w (panel_rescale.cu)
+          acc += (double)sC[k] * (double)__ldg(&mrow[__ldg(&ent[b + k]).x]);
+      }
     }
     // A non-finite u_i (x_i = 0: an empty document) makes the reference's
     // sum over dimensions NaN (fused:382-393).
@@ -431,7 +441,7 @@ static int launch_tc_t(const void* K16, int ld16, float expo, const SourceSel& s
   solve_tc_kernel<NQ><<<(unsigned)grid, kTT, Sh::bytes(cap), st>>>(
       static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr, t.ent,
       t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, cap, ctl.omega,
-      ctl.omega != 1.f ? ctl.vstate : nullptr, out);
+      ctl.omega != 1.f ? ctl.vstate : nullptr, ctl.mrow, out);
   return 1;
 }
 

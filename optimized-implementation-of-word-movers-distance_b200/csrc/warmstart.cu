@@ -178,7 +178,8 @@ __global__ void ws_rows_kernel(const float* __restrict__ E32, int d,
                                const double* __restrict__ u, int ndocs,
                                const int32_t* __restrict__ sel, int G,
                                const int64_t* __restrict__ row0, int F,
-                               float* __restrict__ X, float* __restrict__ y) {
+                               float* __restrict__ X, float* __restrict__ y,
+                               const float* __restrict__ mrow) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (gw >= (int64_t)ndocs * G) return;
@@ -197,8 +198,9 @@ __global__ void ws_rows_kernel(const float* __restrict__ E32, int d,
   const int n = (int)(col_ptr[j + 1] - b);
   float mn = INFINITY, mx = -INFINITY, sm = 0.f;
   for (int k = lane; k < n; k += 32) {
-    const float kv = K[(size_t)ent[b + k].x * ld + i];
-    const float Mv = fmaxf(logf(fmaxf(kv, 1e-38f)) / expo, 0.f);
+    const uint32_t w = ent[b + k].x;
+    const float kv = K[(size_t)w * ld + i];
+    const float Mv = fmaxf(logf(fmaxf(kv, 1e-38f)) / expo, 0.f) + (mrow ? mrow[w] : 0.f);
     mn = fminf(mn, Mv);
     mx = fmaxf(mx, Mv);
     sm += Mv;
@@ -466,12 +468,13 @@ int launch_ws_rows(const float* E32, int d, const float* C, const float* K, int 
                    float expo, const uint32_t* src_ids, const double* r, int vr,
                    const int64_t* col_ptr, const uint2* ent, const int32_t* docs,
                    const double* u, int ndocs, const int32_t* sel, int G,
-                   const int64_t* row0, int F, float* X, float* y, cudaStream_t st) {
+                   const int64_t* row0, int F, float* X, float* y, cudaStream_t st,
+                   const float* mrow) {
   const int64_t threads = (int64_t)ndocs * G * 32;
   if (threads == 0) return 0;
   ws_rows_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
       E32, d, C, K, ld, expo, src_ids, r, vr, col_ptr, ent, docs, u, ndocs, sel, G,
-      row0, F, X, y);
+      row0, F, X, y, mrow);
   return 1;
 }
 

@@ -145,9 +145,12 @@ int launch_gather_sources(const uint32_t* ids, int count, const float* E32,
 
 // FP32 CUDA-core cost panel: K = exp(expo * M), and KM = K * M when KM is
 // not null; M from the GEMM form with near pairs recomputed directly.
+// mrow (row-scaled form, expo != 0): the panel receives M and mrow [V] (set
+// to FLT_MAX bits 0x7f7f7f7f beforehand) the row minima; see panel_rescale.cu.
 int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
                       const SourceSel& s, float expo, float* K, float* KM,
-                      int ld, const NearList& near, cudaStream_t st);
+                      int ld, const NearList& near, cudaStream_t st,
+                      float* mrow = nullptr);
 
 // Tensor-core cost panel (cdist_tc.cu).  Forms: 16-bit operands (E16/S16
 // rows are dp = d rounded up to 8 elements), or the FP32-accurate split-TF32
@@ -164,13 +167,34 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
                     const NearList& near, unsigned* err, int num_sms,
-                    cudaStream_t st);
+                    cudaStream_t st, float* mrow = nullptr);
 
 // Exact FP32 recompute of the listed near pairs (after either cost panel);
 // pairs beyond the list capacity are recomputed by a full-panel scan.
+// scaled: the row-scaled form (the panel holds M; exact M is written).
 int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
                       int ld, uint64_t V, const float* nE, const float* nS,
-                      const uint32_t* vr, int num_sms, cudaStream_t st);
+                      const uint32_t* vr, int num_sms, cudaStream_t st,
+                      bool scaled = false);
+
+// Row-scaled panel (panel_rescale.cu): M -> K' = exp(expo (M - mrow[w])) in
+// place, zero past v_r.  max_norm: the largest squared row norm of E as float
+// bits into *out (device), which decides whether the row-scaled form is used.
+int launch_panel_rescale(float* K, int ld, uint64_t V, const uint32_t* vr,
+                         const float* mrow, float expo, int num_sms, cudaStream_t st);
+int launch_max_norm(const float* nE, uint64_t V, unsigned* out, cudaStream_t st);
+// lambda * M can pass this in a panel row only when the row-scaled form is on.
+constexpr float kScaleLimit = 80.f;
+
+// FP64 re-solve (exact_f64.cu) of the documents whose FP32 result on a
+// row-scaled panel is not finite: lists them (at most exact_f64_list_cap())
+// and solves them again with M recomputed from E32 and the selected rows.
+// Returns launches, -1 if max_doc_len is too long for its shared memory.
+size_t exact_f64_list_cap();
+struct SolveCtl;
+int launch_exact_f64(const float* E32, uint64_t d, const SourceSel& s, const Targets& t,
+                     float expo, const SolveCtl& ctl, int max_doc_len, int32_t* list,
+                     unsigned* count, int num_sms, double* out, cudaStream_t st);
 
 // Iteration control of the solve.  tol <= 0: exactly max_iter x-updates, as
 // the reference (sinkhorn_wmd_fused.cpp:246).  tol > 0: a document stops
@@ -193,6 +217,8 @@ int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
 // document from the cold start unrelaxed (omega = 1 from then on) when the
 // residual is not finite.  Relaxation needs per-document stopping (tol > 0):
 // the caller passes omega = 1 for a fixed update count.
+// mrow: row minima of M of a row-scaled panel (panel_rescale.cu), or null;
+// the final sum then adds c_w * mrow[w] per document word.
 struct SolveCtl {
   int max_iter = 15;
   float tol = 0.f;
@@ -201,6 +227,7 @@ struct SolveCtl {
   int64_t ldu = 0;
   float omega = 1.f;
   float* vstate = nullptr;
+  const float* mrow = nullptr;
 };
 
 constexpr float kRelaxGuard = 100.f;
@@ -321,7 +348,8 @@ int launch_ws_rows(const float* E32, int d, const float* C, const float* K, int 
                    float expo, const uint32_t* src_ids, const double* r, int vr,
                    const int64_t* col_ptr, const uint2* ent, const int32_t* docs,
                    const double* u, int ndocs, const int32_t* sel, int G,
-                   const int64_t* row0, int F, float* X, float* y, cudaStream_t st);
+                   const int64_t* row0, int F, float* X, float* y, cudaStream_t st,
+                   const float* mrow = nullptr);
 int launch_ws_colstats(const float* X, int64_t P, int F, double* s1, double* s2,
                        int chunks, cudaStream_t st);
 int launch_ws_standardize(float* X, int64_t P, int F, const float* shift,
@@ -345,7 +373,7 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
                    const float* S, const float* rinv, int vr, const float* K, int ld,
                    float expo, const Targets& t, const float* Bdoc, float* Asrc,
                    float* u0, int64_t ldu, unsigned* err, int num_sms,
-                   cudaStream_t st);
+                   cudaStream_t st, const float* mrow = nullptr);
 
 // Self-test of the bounded device-side wait (selftest.cu): a wait that can
 // only end through its limit; sets ERR_TIMEOUT in *err.

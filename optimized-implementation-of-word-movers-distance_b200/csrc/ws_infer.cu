@@ -61,6 +61,7 @@ __device__ __forceinline__ uint32_t sw_off(int row, int k, int rows) {
 
 struct Params {
   const float* K;        // FP32 cost panel [V][ld]
+  const float* mrow;     // row minima of M of a row-scaled panel, or null
   int ld;
   float expo;
   const int64_t* col_ptr;
@@ -173,8 +174,10 @@ __global__ void __launch_bounds__(kThreads, 1) ws_init_kernel(const Params p,
       if (ok) {
         const int64_t b = p.col_ptr[j];
         n = (int)(p.col_ptr[j + 1] - b);
-        auto acc = [&](float kv) {
-          const float Mv = fmaxf(__logf(fmaxf(kv, 1e-38f)) / p.expo, 0.f);
+        // M = ln K / expo, plus the row's minimum for a row-scaled panel
+        auto acc = [&](float kv, uint32_t w) {
+          const float Mv = fmaxf(__logf(fmaxf(kv, 1e-38f)) / p.expo, 0.f) +
+                           (p.mrow ? __ldg(&p.mrow[w]) : 0.f);
           lo = fminf(lo, Mv);
           hi = fmaxf(hi, Mv);
           sm += Mv;
@@ -185,12 +188,15 @@ __global__ void __launch_bounds__(kThreads, 1) ws_init_kernel(const Params p,
           const uint32_t w2 = p.ent[b + k + 4].x, w3 = p.ent[b + k + 6].x;
           const float k0 = p.K[(size_t)w0 * p.ld + i], k1 = p.K[(size_t)w1 * p.ld + i];
           const float k2 = p.K[(size_t)w2 * p.ld + i], k3 = p.K[(size_t)w3 * p.ld + i];
-          acc(k0);
-          acc(k1);
-          acc(k2);
-          acc(k3);
+          acc(k0, w0);
+          acc(k1, w1);
+          acc(k2, w2);
+          acc(k3, w3);
         }
-        for (; k < n; k += 2) acc(p.K[(size_t)p.ent[b + k].x * p.ld + i]);
+        for (; k < n; k += 2) {
+          const uint32_t w = p.ent[b + k].x;
+          acc(p.K[(size_t)w * p.ld + i], w);
+        }
       }
       sst[(half * BM + row) * 3 + 0] = lo;
       sst[(half * BM + row) * 3 + 1] = hi;
@@ -361,11 +367,33 @@ int launch_ws_doc_bias(const WsLayout& L, const float* folded, const float* C,
   return 1;
 }
 
+namespace wsi {
+// The iteration is invariant to u -> a u per document (v -> v / a, the same
+// plan and residual), so the prediction fixes u only up to a factor per
+// document.  That factor is set here so that the largest entry of each
+// document's u0 equals the cold start's value v_r: a prediction far off that
+// scale (e.g. every log u near the clamp) would otherwise push v = c / (K^T u)
+// toward the FP32 underflow range.  One warp per document.
+__global__ void ws_scale_kernel(float* __restrict__ u0, int64_t ldu, int vr, int64_t N) {
+  const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= N) return;
+  float* row = u0 + j * ldu;
+  float mx = 0.f;
+  for (int i = lane; i < vr; i += 32) mx = fmaxf(mx, row[i]);
+#pragma unroll
+  for (int off = 16; off; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if (!(mx > 0.f) || !isfinite(mx)) return;  // the solve's fallback judges it
+  const float scale = (float)vr / mx;
+  for (int i = lane; i < vr; i += 32) row[i] *= scale;
+}
+}  // namespace wsi
+
 int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
                    const float* S, const float* rinv, int vr, const float* K, int ld,
                    float expo, const Targets& t, const float* Bdoc, float* Asrc,
                    float* u0, int64_t ldu, unsigned* err, int num_sms,
-                   cudaStream_t st) {
+                   cudaStream_t st, const float* mrow) {
   if (vr <= 0 || t.N <= 0) return 0;
   const float* W1f = folded;
   const float* b1f = W1f + (size_t)kWsH * L.F;
@@ -375,6 +403,7 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
       W1f, L.F, L.d, b1f, S, rinv, vr, Asrc);
   wsi::Params p;
   p.K = K;
+  p.mrow = mrow;
   p.ld = ld;
   p.expo = expo;
   p.col_ptr = t.col_ptr;
@@ -404,7 +433,8 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
   if (grid > ntiles) grid = ntiles;
   const uint32_t idesc = tc::make_idesc(1, wsi::BM, kWsH);
   wsi::ws_init_kernel<<<(unsigned)grid, wsi::kThreads, wsi::smem_bytes(), st>>>(p, idesc);
-  return 2;
+  wsi::ws_scale_kernel<<<(unsigned)((t.N * 32 + 255) / 256), 256, 0, st>>>(u0, ldu, vr, t.N);
+  return 3;
 }
 
 }  // namespace wmd

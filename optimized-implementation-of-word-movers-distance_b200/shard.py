@@ -28,6 +28,25 @@ def partition(col_ptr, parts: int):
     return [(bounds[p], bounds[p + 1]) for p in range(parts)]
 
 
+def partition_sources(vrs, parts: int):
+    """Batched queries: contiguous source ranges [(s0, s1), ...] with about
+    equal sum of v_r each.  A source's solve costs nnz * v_r (every target
+    document against every source word), the target set being the same for
+    all, so v_r is the weight; the split is the prefix-sum search of
+    partition() applied to sources."""
+    w = np.asarray(vrs, np.int64)
+    S = w.size
+    cum = np.concatenate([[0], np.cumsum(w)])
+    total = int(cum[-1])
+    bounds = [0]
+    for p in range(1, parts):
+        target = (total * p) // parts
+        s = int(np.searchsorted(cum, target, side="left"))
+        bounds.append(min(max(s, bounds[-1]), S))
+    bounds.append(S)
+    return [(bounds[p], bounds[p + 1]) for p in range(parts)]
+
+
 def shard_targets(col_ptr, row_inds, vals, j0: int, j1: int):
     """CSC arrays of documents [j0, j1) (column pointers rebased to 0)."""
     col_ptr = np.asarray(col_ptr, np.int64)
@@ -55,6 +74,40 @@ def gather(local, group=None, device=None):
     parts = [torch.empty_like(pad) for _ in range(world)]
     dist.all_gather(parts, pad, group=group)
     return np.concatenate([p[:s].cpu().numpy() for p, s in zip(parts, sizes)])
+
+
+def gather_rows(local, n_cols: int, group=None, device=None):
+    """All ranks' [rows, n_cols] result blocks stacked in rank order."""
+    flat = gather(np.asarray(local, np.float64).reshape(-1), group, device)
+    return flat.reshape(-1, n_cols)
+
+
+class ShardedSources:
+    """One rank's share of a batch of source documents: the embeddings and
+    the whole target set are replicated, the sources [s0, s1) of a
+    v_r-balanced partition are solved on this rank's GPU, and `query_batch`
+    returns every source's scores (local batch + gather)."""
+
+    def __init__(self, vecs, col_ptr, row_inds, vals, rank: int, world: int,
+                 device: int = 0):
+        from . import Engine
+        self.rank, self.world, self.device = rank, world, device
+        self.N = len(col_ptr) - 1
+        self.eng = Engine(device)
+        self.eng.set_embeddings(vecs)
+        self.eng.set_targets(col_ptr, row_inds, vals)
+
+    def query_batch(self, sources, lam: float, max_iter: int, group=None):
+        import torch
+        vrs = [int(np.count_nonzero(r)) if np.ndim(r) == 1 else len(r[0])
+               for r in sources]
+        s0, s1 = partition_sources(vrs, self.world)[self.rank]
+        local = (self.eng.query_batch(list(sources[s0:s1]), lam, max_iter)
+                 if s1 > s0 else np.zeros((0, self.N)))
+        return gather_rows(local, self.N, group, torch.device("cuda", self.device))
+
+    def close(self):
+        self.eng.close()
 
 
 class ShardedEngine:

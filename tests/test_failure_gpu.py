@@ -45,16 +45,22 @@ def test_bounded_wait_gives_up_and_handle_recovers(wmd, synth, oracle_mod):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "bf16"])
-@pytest.mark.parametrize("kind", ["non_finite", "wild"])
+@pytest.mark.parametrize("kind", ["constant", "wild"])
 def test_warm_start_fallback_to_cold_start(wmd, synth, prec, kind):
+    """'wild': finite, wildly varying predictions; every document must fall
+    back, giving the cold start's results and counts bit for bit.
+    'constant': a huge constant prediction (every log u at its clamp): the
+    same point as the cold start up to the scale the iteration ignores, so
+    the results must agree with the cold start's within the stopping
+    tolerance, in about as many updates."""
     p = synth.case(3000, 300, 200, 24, 8, 96, 40, 31)
     held = [synth.source_doc(p.V, v, seed=700 + v) for v in (20, 48, 120)]
     F, o, _ = ws_mlp.layout(300)
     params = wmd.ws_init_params(300, 5).copy()
     a3, _ = o["b3"]
     aw, mw = o["w3"]
-    if kind == "non_finite":
-        params[a3] = 1.0e4  # u0 = exp(1e4) = inf for every pair
+    if kind == "constant":
+        params[a3] = 1.0e4  # log u clamped to its upper bound for every pair
     else:
         # finite but wildly varying log u per (word, document)
         rng = np.random.default_rng(9)
@@ -71,6 +77,12 @@ def test_warm_start_fallback_to_cold_start(wmd, synth, prec, kind):
         assert np.isfinite(u0).mean() > 0.5  # the prediction itself is finite
     warm, it_warm = eng.query_batch(held, p.lam, 3000, want_iters=True)
     eng.close()
-    assert np.array_equal(it_warm, it_cold)
-    same = (warm == cold) | (np.isnan(warm) & np.isnan(cold))
-    assert same.all(), f"{(~same).sum()} documents differ from the cold start"
+    if kind == "wild":
+        assert np.array_equal(it_warm, it_cold)
+        same = (warm == cold) | (np.isnan(warm) & np.isnan(cold))
+        assert same.all(), f"{(~same).sum()} documents differ from the cold start"
+    else:
+        done = (it_warm < 3000) & (it_cold < 3000)
+        assert done.mean() > 0.98
+        assert abs(it_warm.mean() - it_cold.mean()) <= 0.02 * it_cold.mean()
+        assert rel_err(warm[done], cold[done]).max() <= 1e-4

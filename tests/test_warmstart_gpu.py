@@ -107,8 +107,14 @@ def test_inference_vs_cpu_oracle(wmd, small):
     X = ws_mlp.features(p.vecs, p.col_ptr, p.row_inds, p.vals, ids, r[ids], pairs)
     y, _ = ws_mlp.forward(params.astype(np.float64), 300, X)
     got = np.log(np.array([u0[j, i] for i, j in pairs], np.float64))
-    err = np.abs(got - y)
-    assert err.max() <= 0.05 + 0.01 * np.abs(y).max(), err.max()
+    # u0 is the prediction up to one factor per document (the iteration is
+    # invariant to it; the engine sets it so that the largest entry is v_r):
+    # compare per-document centred log u, and the largest entry.
+    nw = ids.size
+    g2, y2 = got.reshape(-1, nw), y.reshape(-1, nw)
+    err = np.abs((g2 - g2.mean(1, keepdims=True)) - (y2 - y2.mean(1, keepdims=True)))
+    assert err.max() <= 2 * (0.05 + 0.01 * np.abs(y).max()), err.max()
+    assert np.allclose(np.exp(g2).max(1), nw, rtol=1e-5)
     eng.close()
 
 
