@@ -387,6 +387,20 @@ def extras(a, wmd, p, dev):
                                                 "median": float(np.median(e15))},
                        "rel_err_vs_converged_fp64": {"max": float(ec.max()),
                                                      "median": float(np.median(ec))}}
+    # the reference's word-major traversal on the GPU (FP32-accurate cost
+    # panel, each K row streamed once per pass, u / x gathered and scattered
+    # per entry) against the document-major solve above
+    eng.set_cdist_mode("tf32x3")
+    eng.set_solve_order("word")
+    fn = lambda: eng.query_device(r_dev.data_ptr(), W["v_r"], p.lam, p.max_iter,
+                                  o.data_ptr())
+    dt = timed(eng, fn, 20)
+    e15 = _rel(o[:sub].cpu().numpy(), ref15)
+    forms["tf32x3_word_major"] = {"pairs_per_s": p.N / dt,
+                                  "rel_err_vs_fp64_15it": {"max": float(e15.max())},
+                                  "vs_document_major": (p.N / dt) /
+                                  forms["tf32x3"]["pairs_per_s"]}
+    eng.set_solve_order("document")
     out["single_source_forms"] = forms
     # 2. converged criterion: marginal residual <= 1e-4 per document (WMD
     #    within ~6e-5 of the converged FP64 oracle), cap 5000 updates
@@ -601,6 +615,23 @@ def large_vocab(wmd, dev):
         "panel read once per source (nnz * ld16 * 2), the minimum the solve "
         "must stream from HBM", "achieved_gbs": gbs, "peak_gbs": peak,
         "frac": gbs / peak, "peak_source": src}
+    # the panel beyond L2: the reference's word-major order (each K row
+    # streamed once per pass, u / x through HBM) against the document-major
+    # FP32 solve, one source each, device time
+    eng.set_solve_precision("fp32")
+    wm = {}
+    for order in ("document", "word"):
+        eng.set_solve_order(order)
+        eng.set_timing(True)
+        o1 = eng.query(rs[0], 10.0, 15)
+        sel, cd, sv = eng.stage_times()
+        wm[order] = {"solve_ms": sv, "pairs_per_s_solve": N / (sv * 1e-3)}
+        if order == "document":
+            o_doc = o1
+    eng.set_solve_order("document")
+    wm["word"]["max_rel_diff_vs_document"] = float(np.nanmax(_rel(o1, o_doc)))
+    wm["v_r"] = int(vrs[0])
+    res["solve_order_one_source"] = wm
     # at the converged criterion (marginal residual <= 1e-4, WMD within
     # ~6e-5 of the converged FP64 value): the plain FP32 path against the
     # BF16 panel with both half-steps over-relaxed

@@ -172,6 +172,16 @@ typedef enum wmd_solve_precision {
 } wmd_solve_precision;
 wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec);
 
+/* Traversal order of the iterations.  0 (default): document-major, a
+ * document's u and x on chip for all passes (solve.cu, solve_block.cu).
+ * 1: word-major, the reference's own order (sinkhorn_wmd_fused.cpp:249-292:
+ * nnz-balanced chunks of the word-major CSR, each K row read once per pass,
+ * u gathered and x scattered with atomics per entry); the fixed update count
+ * from the cold start only (no tolerance, relaxation or warm start, lambda
+ * != 0), single-source queries only.  Results agree with order 0 within the
+ * plain path's tolerance (atomic summation order). */
+wmd_status wmd_set_solve_order(wmd_handle* h, int order);
+
 /* Launch-shape autotuner of the BF16 block solve (on by default): the first
  * solve of each panel width (and panel size class: within / beyond 64 MiB)
  * times every candidate shape on the handle's real data and keeps the

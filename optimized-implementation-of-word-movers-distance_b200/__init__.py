@@ -318,6 +318,13 @@ class Engine:
         for sources with 64 < v_r <= 512."""
         check(lib().wmd_set_solve_precision(self._h, {"fp32": 0, "bf16": 1}[prec]))
 
+    def set_solve_order(self, order: str):
+        """'document' (default: a document's scalings on chip for every pass)
+        or 'word' (the reference's word-major traversal: each K row read once
+        per pass, u gathered and x scattered per entry; fixed update count,
+        cold start, single-source queries)."""
+        check(lib().wmd_set_solve_order(self._h, {"document": 0, "word": 1}[order]))
+
     def query(self, r, lam: float, max_iter: int) -> np.ndarray:
         r = _f64(r)
         out = np.empty(self.N, np.float64)

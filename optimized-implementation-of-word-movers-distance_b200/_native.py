@@ -69,6 +69,7 @@ _SIGS = [
     ("wmd_set_targets_csr", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSR)]),
     ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_solve_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("wmd_set_solve_order", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_relaxation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     ("wmd_autotune_choices", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),

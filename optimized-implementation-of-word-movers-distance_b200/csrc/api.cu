@@ -95,13 +95,13 @@ struct QueryKey {
   float tol = 0.f;
   float omega = 1.f;
   int prec = -1;
-  const void* bufs[18] = {};  // every device buffer the graph reads or writes
+  const void* bufs[24] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
           epoch == o.epoch && tol == o.tol && omega == o.omega && prec == o.prec))
       return false;
-    for (int i = 0; i < 18; ++i)
+    for (int i = 0; i < 24; ++i)
       if (bufs[i] != o.bufs[i]) return false;
     return true;
   }
@@ -148,6 +148,11 @@ struct wmd_handle {
   DevBuf mrow, emax_dev;
   float emax2 = 0.f;
   DevBuf exact_list, exact_count;  // documents re-solved in FP64 (exact_f64.cu)
+  // Word-major solve order (solve_word.cu): the target set as word-major CSR
+  // (built on first use per target set) and the u / x state it streams.
+  int solve_order = 0;  // 0 document-major, 1 word-major
+  bool wm_ready = false;
+  DevBuf wm_rp, wm_ent, wm_u, wm_x;
   // batched queries
   DevBuf b_ids, b_rinv, b_vr, b_out, b_iters;
   // Second pipeline slot of the batched queries (its own stream and
@@ -155,7 +160,7 @@ struct wmd_handle {
   // one source's solve tail overlaps the next source's cost panel and solve.
   struct BatchSlot {
     DevBuf sel_S, sel_nS, sel_S16, near_pairs, near_count, K, KM, K16, vstate,
-        ws_Asrc, ws_u0, mrow, exact_list, exact_count;
+        ws_Asrc, ws_u0, ws_stats, mrow, exact_list, exact_count;
   } slot1;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t join[2] = {nullptr, nullptr};
@@ -163,7 +168,7 @@ struct wmd_handle {
   DevBuf topk_scratch, topk_idx, topk_val;
   // learned warm start: model (FP32 parameters, folded inference form),
   // per-target-set tables, per-query scratch
-  DevBuf ws_params, ws_folded, ws_C, ws_Bdoc, ws_Asrc, ws_u0;
+  DevBuf ws_params, ws_folded, ws_C, ws_Bdoc, ws_Asrc, ws_u0, ws_stats;
   bool ws_on = false;       // queries start from the model's prediction
   bool ws_docs_ready = false;  // ws_C / ws_Bdoc match targets + model
   int ws_d = 0;
@@ -357,6 +362,7 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   h->N = N;
   h->nnz = nnz;
   h->have_T = true;
+  h->wm_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
   for (auto& row : h->tc_long)
@@ -502,10 +508,50 @@ wmd_status ws_prepare_docs(wmd_handle* h) {
   return WMD_OK;
 }
 
+// Word-major CSR of the resident target set (stable: documents ascending
+// within a word), from the device's document-major entries; once per target
+// set, synchronising.
+wmd_status build_word_major(wmd_handle* h) {
+  const uint64_t N = h->N, nnz = h->nnz, V = h->tV;
+  std::vector<int64_t> cp(N + 1);
+  std::vector<uint2> ent(nnz);
+  CK(cudaMemcpyAsync(cp.data(), h->col_ptr.p, (N + 1) * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (nnz)
+    CK(cudaMemcpyAsync(ent.data(), h->ent.p, nnz * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  std::vector<int64_t> rp(V + 1, 0);
+  for (uint64_t e = 0; e < nnz; ++e) rp[ent[e].x + 1]++;
+  for (uint64_t w = 0; w < V; ++w) rp[w + 1] += rp[w];
+  std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
+  std::vector<uint2> went(std::max<uint64_t>(nnz, 1));
+  for (uint64_t j = 0; j < N; ++j)
+    for (int64_t e = cp[j]; e < cp[j + 1]; ++e)
+      went[pos[ent[e].x]++] = make_uint2((unsigned)j, ent[e].y);
+  CK(h->wm_rp.ensure((V + 1) * 8));
+  CK(h->wm_ent.ensure(std::max<uint64_t>(nnz, 1) * 8));
+  CK(cudaMemcpyAsync(h->wm_rp.p, rp.data(), (V + 1) * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->wm_ent.p, went.data(), std::max<uint64_t>(nnz, 1) * 8,
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
+  h->wm_ready = true;
+  h->graph_epoch++;
+  return WMD_OK;
+}
+
 // One query on device-resident r.  cap bounds v_r.  expo: K = exp(expo * M).
 wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
                         float expo, int max_iter, double* out_dev) {
   const uint64_t V = h->V, d = h->d;
+  const bool word_major = h->solve_order == 1;
+  if (word_major) {
+    if (h->tol > 0.f || h->omega != 1.f || h->ws_on || expo == 0.f)
+      return fail(WMD_ERR_UNSUPPORTED, "the word-major order runs the fixed update "
+                                       "count from the cold start, unrelaxed, lambda != 0");
+    if (!h->wm_ready) {
+      wmd_status sw = build_word_major(h);
+      if (sw) return sw;
+    }
+  }
   const int nchunks = select_num_chunks(V);
   const int ld = (int)(((cap ? cap : 1) + 3u) & ~3u);
   CK(h->sel_ids.ensure((size_t)std::max<uint32_t>(cap, 1) * sizeof(uint32_t)));
@@ -519,8 +565,16 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   const bool need_km = expo == 0.f;
   if (need_km) CK(h->KM.ensure((size_t)V * ld * sizeof(float)));
   float* KMp = need_km ? h->KM.as<float>() : nullptr;
-  const int ld16 = h->prec == WMD_SOLVE_BF16 && !need_km ? block_panel_width(cap) : 0;
+  // The row-scaled form (lambda * M beyond FP32's range) keeps the FP32
+  // panel: BF16 rounding of K' is amplified there.
+  const int ld16 = h->prec == WMD_SOLVE_BF16 && !need_km && !word_major &&
+                           !row_scaled(h, expo)
+                       ? block_panel_width(cap) : 0;
   if (ld16) CK(h->K16.ensure((size_t)V * ld16 * 2));
+  if (word_major) {
+    CK(h->wm_u.ensure((size_t)std::max<uint64_t>(h->N, 1) * ld * sizeof(float)));
+    CK(h->wm_x.ensure((size_t)std::max<uint64_t>(h->N, 1) * ld * sizeof(float)));
+  }
   SourceSel sel;
   sel.ids = h->sel_ids.as<uint32_t>();
   sel.rinv = h->sel_rinv.as<float>();
@@ -585,6 +639,8 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     if (sw) return sw;
     CK(h->ws_Asrc.ensure((size_t)std::max<uint32_t>(cap, 1) * kWsH * sizeof(float)));
     CK(h->ws_u0.ensure((size_t)std::max<uint64_t>(h->N, 1) * ld * sizeof(float)));
+    CK(h->ws_stats.ensure((size_t)std::max<uint64_t>(h->N, 1) * std::max<uint32_t>(cap, 1) *
+                          3 * sizeof(float)));
   }
   // Everything below is stream work only (no allocation, no host sync), so
   // it can be captured into a CUDA graph and replayed.
@@ -635,12 +691,25 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
                           h->ws_params.as<float>(), sel.S, sel.rinv, (int)cap,
                           h->K.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
                           h->ws_Asrc.as<float>(), h->ws_u0.as<float>(), ld,
-                          h->err_dev.as<unsigned>(), h->sms, h->stream, mrow);
+                          h->err_dev.as<unsigned>(), h->sms, h->stream, mrow,
+                          h->ws_stats.as<float>());
       ctl.u0 = h->ws_u0.as<float>();
       ctl.ldu = ld;
     }
     CK(record(2, capturing));
-    if (ld16) {
+    if (word_major) {
+      WordMajor wm;
+      wm.row_ptr = h->wm_rp.as<int64_t>();
+      wm.ent = h->wm_ent.as<uint2>();
+      wm.V = (int64_t)V;
+      wm.nnz = (int64_t)h->nnz;
+      wm.mrow = mrow;
+      const int lw = launch_solve_word(h->K.as<float>(), ld, expo, cap, sel, wm,
+                                       (int64_t)h->N, max_iter, h->wm_u.as<float>(),
+                                       h->wm_x.as<float>(), h->sms, out_dev, h->stream);
+      if (lw < 0) return fail(WMD_ERR_UNSUPPORTED, "more than 1024 source words");
+      n += lw;
+    } else if (ld16) {
       n += launch_panel_to_bf16(h->K.as<float>(), ld, h->K16.p, ld16, V, sel.vr,
                                 h->sms, h->stream);
       const int shape = block_shape_for(h, h->K16.p, ld16, expo, cap, sel, t, ctl,
@@ -683,11 +752,14 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.omega = h->omega;
   key.prec = (int)h->prec + (ws ? 2 : 0);
   {
-    const DevBuf* used[18] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+    const DevBuf* used[24] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
                               &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
                               &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16,
-                              &h->ws_Asrc, &h->ws_u0, &h->vstate, &h->mrow};
-    for (int i = 0; i < 18; ++i) key.bufs[i] = used[i]->p;
+                              &h->ws_Asrc, &h->ws_u0, &h->vstate, &h->mrow,
+                              &h->ws_stats, &h->exact_list, &h->exact_count,
+                              &h->wm_u, &h->wm_x, &h->wm_ent};
+    for (int i = 0; i < 24; ++i) key.bufs[i] = used[i]->p;
+    key.prec += word_major ? 16 : 0;
   }
   if (!h->use_graphs) {
     int n = 0;
@@ -802,6 +874,8 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                        float expo, int max_iter, double* wmd_out, int* iters_out) {
   if (!h->have_E || !h->have_T)
     return fail(WMD_ERR_INVALID_ARG, "embeddings and targets must be set first");
+  if (h->solve_order != 0)
+    return fail(WMD_ERR_UNSUPPORTED, "batched queries run document-major only");
   if (h->tV != h->V)
     return fail(WMD_ERR_INVALID_ARG, "target rows != vocabulary size");
   if (!src_ptr || S == 0 || !wmd_out) return fail(WMD_ERR_INVALID_ARG, "bad batch");
@@ -868,6 +942,7 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     if (sw) return sw;
     CK(h->ws_Asrc.ensure((size_t)vr_max * kWsH * sizeof(float)));
     CK(h->ws_u0.ensure((size_t)std::max<uint64_t>(N, 1) * ld_max * sizeof(float)));
+    CK(h->ws_stats.ensure((size_t)std::max<uint64_t>(N, 1) * vr_max * 3 * sizeof(float)));
   }
   const unsigned near_cap = (unsigned)std::min<uint64_t>((uint64_t)V * vr_max, 1u << 20);
   CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
@@ -890,6 +965,7 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     if (ws) {
       CK(b1.ws_Asrc.ensure((size_t)vr_max * kWsH * sizeof(float)));
       CK(b1.ws_u0.ensure((size_t)std::max<uint64_t>(N, 1) * ld_max * sizeof(float)));
+      CK(b1.ws_stats.ensure((size_t)std::max<uint64_t>(N, 1) * vr_max * 3 * sizeof(float)));
     }
     CK(b1.near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
     CK(b1.near_count.ensure(sizeof(unsigned)));
@@ -947,6 +1023,7 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
     DevBuf& bVS = in1 ? h->slot1.vstate : h->vstate;
     DevBuf& bAs = in1 ? h->slot1.ws_Asrc : h->ws_Asrc;
     DevBuf& bU0 = in1 ? h->slot1.ws_u0 : h->ws_u0;
+    DevBuf& bSt = in1 ? h->slot1.ws_stats : h->ws_stats;
     float* KMs = need_km ? (in1 ? h->slot1.KM : h->KM).as<float>() : nullptr;
     float* mrow = scaled ? (in1 ? h->slot1.mrow : h->mrow).as<float>() : nullptr;
     SourceSel sel;
@@ -1002,11 +1079,12 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                                  h->ws_params.as<float>(), sel.S, sel.rinv, (int)vr,
                                  bK.as<float>(), ld, expo, t, h->ws_Bdoc.as<float>(),
                                  bAs.as<float>(), bU0.as<float>(), ld,
-                                 h->err_dev.as<unsigned>(), h->sms, sst, mrow);
+                                 h->err_dev.as<unsigned>(), h->sms, sst, mrow,
+                                 bSt.as<float>());
       ctl.u0 = bU0.as<float>();
       ctl.ldu = ld;
     }
-    const int ld16 = h->prec == WMD_SOLVE_BF16 && !KMs ? block_panel_width(vr) : 0;
+    const int ld16 = h->prec == WMD_SOLVE_BF16 && !KMs && !mrow ? block_panel_width(vr) : 0;
     int ls;
     if (ld16) {
       launches += launch_panel_to_bf16(bK.as<float>(), ld, bK16.p, ld16, V, sel.vr,
@@ -1390,6 +1468,14 @@ wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes) {
 }
 
 const char* wmd_block_shape_name(int shape) { return block_shape_name(shape); }
+
+wmd_status wmd_set_solve_order(wmd_handle* h, int order) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (order != 0 && order != 1) return fail(WMD_ERR_INVALID_ARG, "order must be 0 or 1");
+  h->solve_order = order;
+  h->graph_epoch++;
+  return WMD_OK;
+}
 
 wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
@@ -2063,6 +2149,7 @@ wmd_status wmd_set_targets_edges(wmd_handle* h, const uint64_t* words,
   h->N = N;
   h->nnz = nnz;
   h->have_T = true;
+  h->wm_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
   for (auto& row : h->tc_long)

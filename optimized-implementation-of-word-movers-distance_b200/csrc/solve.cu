@@ -624,6 +624,11 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     for (int t = 0; t < 16; ++t) {
       const int d0 = 32 * q + 2 * t;
       bad |= (d0 < vr && !isfinite(u2[t].x)) || (d0 + 1 < vr && !isfinite(u2[t].y));
+      // Row-scaled panel: a u this large means a source word whose K entries
+      // in this document are at the FP32 floor (subnormal, few significant
+      // bits): the document goes to the FP64 re-solve (exact_f64.cu).
+      if (mrow)
+        bad |= (d0 < vr && u2[t].x > kScaledUMax) || (d0 + 1 < vr && u2[t].y > kScaledUMax);
     }
     if (__any_sync(0xffffffffu, bad)) acc = __longlong_as_double(0x7ff8000000000000ll);
     if (vr == 0) acc = 0.0;  // no source word: an empty sum (fused:387)

@@ -379,7 +379,8 @@ solve_tc_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     // A non-finite u_i (x_i = 0: an empty document) makes the reference's
     // sum over dimensions NaN (fused:382-393).
     bool bad = false;
-    for (int D = tid; D < vr; D += kTT) bad |= !isfinite(cur[D]);
+    for (int D = tid; D < vr; D += kTT)
+      bad |= !isfinite(cur[D]) || (mrow && cur[D] > kScaledUMax);  // see solve.cu
     __syncthreads();  // every warp has read the last u before red is reused
     if (lane == 0) red[warp] = acc;
     bad = __syncthreads_or(bad);

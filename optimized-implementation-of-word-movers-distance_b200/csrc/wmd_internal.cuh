@@ -185,6 +185,10 @@ int launch_panel_rescale(float* K, int ld, uint64_t V, const uint32_t* vr,
 int launch_max_norm(const float* nE, uint64_t V, unsigned* out, cudaStream_t st);
 // lambda * M can pass this in a panel row only when the row-scaled form is on.
 constexpr float kScaleLimit = 80.f;
+// On a row-scaled panel, a final scaling u_i above this marks a document
+// whose K entries for source word i sit at the FP32 floor; it is re-solved
+// in FP64 with the non-finite ones.
+constexpr float kScaledUMax = 1e30f;
 
 // FP64 re-solve (exact_f64.cu) of the documents whose FP32 result on a
 // row-scaled panel is not finite: lists them (at most exact_f64_list_cap())
@@ -303,6 +307,20 @@ int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
                  const SolveCtl& ctl, double* out, cudaStream_t st);
 
+// Word-major solve (solve_word.cu): the reference's traversal order, each K
+// row read once per pass, u gathered and x scattered (atomics) per entry.
+// Fixed update count, cold start, unrelaxed.  ent: {document, float bits of
+// c} in word-major order, row_ptr [V+1].  u, x: scratch [N][ld].
+struct WordMajor {
+  const int64_t* row_ptr = nullptr;
+  const uint2* ent = nullptr;
+  int64_t V = 0, nnz = 0;
+  const float* mrow = nullptr;  // row-scaled panel, or null
+};
+int launch_solve_word(const float* K, int ld, float expo, uint32_t vr_cap,
+                      const SourceSel& s, const WordMajor& wm, int64_t N, int max_iter,
+                      float* u, float* x, int num_sms, double* out, cudaStream_t st);
+
 // Wide-source solve (solve_block.cu): one CTA per document over a BF16 panel
 // [V][ld16], ld16 = block_panel_width(v_r) (0: not applicable).  u0, when
 // not null, is an initial scaling [N][ldu] (warm start, cold fallback).
@@ -373,7 +391,10 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
                    const float* S, const float* rinv, int vr, const float* K, int ld,
                    float expo, const Targets& t, const float* Bdoc, float* Asrc,
                    float* u0, int64_t ldu, unsigned* err, int num_sms,
-                   cudaStream_t st, const float* mrow = nullptr);
+                   cudaStream_t st, const float* mrow = nullptr,
+                   float* stats = nullptr);
+// stats: scratch [N][vr][3] for the per-pair M statistics (computed
+// document-major first); null: the fused kernel walks the panel per pair.
 
 // Self-test of the bounded device-side wait (selftest.cu): a wait that can
 // only end through its limit; sets ERR_TIMEOUT in *err.

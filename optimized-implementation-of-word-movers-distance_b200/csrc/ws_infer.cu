@@ -10,8 +10,10 @@
 //   z1 = A_i + B_j + W_s [min M, mean M, max M]_ij
 //   A_i = W1f_E E_i + W1f_r r_i + W1f_lr log r_i + b1f   (per source word)
 //   B_j = W1f_C centroid_j                                (per document)
-// Only the three M statistics are per pair; they are read from the cost
-// panel at the document's words (M = ln K / expo) by the same kernel.
+// Only the three M statistics are per pair.  ws_stats_kernel computes them
+// first, document-major (one warp per document, lanes over the source words:
+// every K row of the document is read once, coalesced), into a [N][v_r][3]
+// table that the fused kernel reads in its own pair order.
 //
 // Per 128-pair tile (pairs in document-major order p = j * v_r + i):
 //   warps 1-8  stats + z1 + GELU, written as BF16 straight into shared memory
@@ -62,6 +64,7 @@ __device__ __forceinline__ uint32_t sw_off(int row, int k, int rows) {
 struct Params {
   const float* K;        // FP32 cost panel [V][ld]
   const float* mrow;     // row minima of M of a row-scaled panel, or null
+  const float* stats;    // [N][vr][3] min / mean / max of M per pair
   int ld;
   float expo;
   const int64_t* col_ptr;
@@ -171,7 +174,17 @@ __global__ void __launch_bounds__(kThreads, 1) ws_init_kernel(const Params p,
       // in flight each, and combine through shared memory.
       int n = 0;
       float lo = INFINITY, hi = -INFINITY, sm = 0.f;
-      if (ok) {
+      if (ok && p.stats) {
+        // precomputed (ws_stats_kernel): half 0 takes the pair's values,
+        // half 1 the neutral ones, so the combine below is unchanged
+        n = (int)(p.col_ptr[j + 1] - p.col_ptr[j]);
+        if (half == 0 && n > 0) {
+          const float* st = p.stats + (size_t)pr * 3;
+          lo = st[0];
+          sm = st[1] * (float)n;
+          hi = st[2];
+        }
+      } else if (ok) {
         const int64_t b = p.col_ptr[j];
         n = (int)(p.col_ptr[j + 1] - b);
         // M = ln K / expo, plus the row's minimum for a row-scaled panel
@@ -368,6 +381,44 @@ int launch_ws_doc_bias(const WsLayout& L, const float* folded, const float* C,
 }
 
 namespace wsi {
+// Per (document j, source word i): min / mean / max over j's words w of
+// M = ln K[w][i] / expo (+ mrow[w] for a row-scaled panel), one warp per
+// document, lanes over i: the document's K rows are read once and coalesced.
+__global__ void ws_stats_kernel(const float* __restrict__ K, int ld, float expo,
+                                const float* __restrict__ mrow,
+                                const int64_t* __restrict__ col_ptr,
+                                const uint2* __restrict__ ent, int vr, int64_t N,
+                                float* __restrict__ stats) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t j = w0; j < N; j += nw) {
+    const int64_t b = col_ptr[j];
+    const int n = (int)(col_ptr[j + 1] - b);
+    for (int i0 = 0; i0 < vr; i0 += 32) {
+      const int i = i0 + lane;
+      float lo = INFINITY, hi = -INFINITY, sm = 0.f;
+      for (int k = 0; k < n; ++k) {
+        const uint32_t w = __ldg(&ent[b + k]).x;
+        if (i < vr) {
+          const float kv = __ldg(&K[(size_t)w * ld + i]);
+          const float Mv = fmaxf(__logf(fmaxf(kv, 1e-38f)) / expo, 0.f) +
+                           (mrow ? __ldg(&mrow[w]) : 0.f);
+          lo = fminf(lo, Mv);
+          hi = fmaxf(hi, Mv);
+          sm += Mv;
+        }
+      }
+      if (i < vr) {
+        float* st = stats + ((size_t)j * vr + i) * 3;
+        st[0] = n > 0 ? lo : 0.f;
+        st[1] = n > 0 ? sm / (float)n : 0.f;
+        st[2] = n > 0 ? hi : 0.f;
+      }
+    }
+  }
+}
+
 // The iteration is invariant to u -> a u per document (v -> v / a, the same
 // plan and residual), so the prediction fixes u only up to a factor per
 // document.  That factor is set here so that the largest entry of each
@@ -393,8 +444,15 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
                    const float* S, const float* rinv, int vr, const float* K, int ld,
                    float expo, const Targets& t, const float* Bdoc, float* Asrc,
                    float* u0, int64_t ldu, unsigned* err, int num_sms,
-                   cudaStream_t st, const float* mrow) {
+                   cudaStream_t st, const float* mrow, float* stats) {
   if (vr <= 0 || t.N <= 0) return 0;
+  if (stats) {
+    int64_t g = (t.N * 32 + 255) / 256;
+    const int64_t cap = (int64_t)(num_sms > 0 ? num_sms : 148) * 16;
+    if (g > cap) g = cap;
+    wsi::ws_stats_kernel<<<(unsigned)g, 256, 0, st>>>(K, ld, expo, mrow, t.col_ptr,
+                                                       t.ent, vr, t.N, stats);
+  }
   const float* W1f = folded;
   const float* b1f = W1f + (size_t)kWsH * L.F;
   const float* Ws = b1f + kWsH;
@@ -404,6 +462,7 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
   wsi::Params p;
   p.K = K;
   p.mrow = mrow;
+  p.stats = stats;
   p.ld = ld;
   p.expo = expo;
   p.col_ptr = t.col_ptr;
@@ -434,7 +493,7 @@ int launch_ws_init(const WsLayout& L, const float* folded, const float* params,
   const uint32_t idesc = tc::make_idesc(1, wsi::BM, kWsH);
   wsi::ws_init_kernel<<<(unsigned)grid, wsi::kThreads, wsi::smem_bytes(), st>>>(p, idesc);
   wsi::ws_scale_kernel<<<(unsigned)((t.N * 32 + 255) / 256), 256, 0, st>>>(u0, ldu, vr, t.N);
-  return 3;
+  return stats ? 4 : 3;
 }
 
 }  // namespace wmd

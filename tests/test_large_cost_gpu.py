@@ -11,7 +11,9 @@ agree with it.
 
 Tolerance: 1e-4 relative.  At these sizes M itself is ~20-30 and its FP32
 rounding alone moves K by lambda * ulp(M) ~ 2e-5 relative, so the plain
-path's 1e-5 does not apply; alpha = 1 (lambda M <= 32) keeps 1e-5.
+path's 1e-5 does not apply; alpha = 1 (lambda M <= 32) keeps 1e-5 (1e-4 for
+the BF16 panel, its usual bar).  In the row-scaled form the engine keeps the
+FP32 panel even when the BF16 one is requested.
 """
 import numpy as np
 import pytest
@@ -50,7 +52,8 @@ def test_large_lambda_m_vs_oracle(wmd, synth, oracle_mod, alpha, v_r, prec):
     got = eng.query(p.r, p.lam, p.max_iter)
     eng.close()
     assert np.isfinite(got).all(), f"{(~np.isfinite(got)).sum()} documents not finite"
-    tol = 1e-5 if alpha == 1.0 else (1e-4 if prec == "fp32" else 2e-4)
+    # BF16 panel (alpha = 1): its own 1e-4 bar; alpha >= 3 runs the FP32 panel
+    tol = 1e-5 if (alpha == 1.0 and prec == "fp32") else 1e-4
     err = rel_err(got, ref)
     assert err.max() <= tol, f"max rel err {err.max():.3e}"
 
