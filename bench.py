@@ -487,12 +487,20 @@ def batched_sections(a, wmd, p, dev):
                       for r in rs[:samp_src]])
     for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
         eng.set_solve_precision(prec)
-        eng.query_batch(_one_per_width(rs), lam, 15)  # launch-shape tuning
-        res, dt = _device_batch(eng, rs, lam, 15)
-        e = _rel(res[:samp_src, :samp_docs], ref15)
-        batched[name] = {"pairs_per_s": S * N / dt, "seconds": dt,
-                         "rel_err_vs_fp64_15it": {"max": float(np.nanmax(e)),
-                                                  "median": float(np.nanmedian(e))}}
+        # stacked groups (the default: a fixed number of launches per group of
+        # same-width sources) and, for comparison, source by source
+        for stacked in (True, False):
+            eng.set_batch_mode(stacked)
+            eng.query_batch(_one_per_width(rs), lam, 15)  # launch-shape tuning
+            res, dt = _device_batch(eng, rs, lam, 15)
+            e = _rel(res[:samp_src, :samp_docs], ref15)
+            key = name if stacked else name + "_per_source"
+            batched[key] = {"pairs_per_s": S * N / dt, "seconds": dt,
+                            "launches": eng.launch_count,
+                            "groups": eng.last_batch_groups,
+                            "rel_err_vs_fp64_15it": {"max": float(np.nanmax(e)),
+                                                     "median": float(np.nanmedian(e))}}
+        eng.set_batch_mode(True)
     batched["bf16_panel"]["speedup_vs_plain_fp32"] = (
         batched["plain_fp32"]["seconds"] / batched["bf16_panel"]["seconds"])
     batched["bf16_panel"]["autotuned_shapes"] = {

@@ -182,6 +182,31 @@ wmd_status wmd_set_solve_precision(wmd_handle* h, wmd_solve_precision prec);
  * plain path's tolerance (atomic summation order). */
 wmd_status wmd_set_solve_order(wmd_handle* h, int order);
 
+/* Batched queries (wmd_query_batch), no reference counterpart.  stacked != 0
+ * (the default): sources of one width class (lane layout of the warp solve,
+ * or BF16 panel width of the CTA-per-document solve) run in groups whose
+ * panels fit group_budget_bytes of device memory (default 32 GiB), each group
+ * in a fixed number of launches whatever its size: one gather of all the
+ * group's source rows, one tensor-core cost-panel launch writing every
+ * source's panel, one near-pair fix-up, (BF16) one panel conversion, and one
+ * persistent solve launch over all (source, document) pairs.  Used with a
+ * tensor-core cost panel, lambda != 0, the cold start and panels in FP32
+ * range; otherwise (and with stacked = 0) sources run one after another on
+ * two pipeline slots.  Results are the same either way (same kernels' math). */
+wmd_status wmd_set_batch_mode(wmd_handle* h, int stacked, uint64_t group_budget_bytes);
+
+/* Number of stacked groups the last wmd_query_batch ran (0: per source). */
+int wmd_last_batch_groups(wmd_handle* h);
+
+/* Launch shapes the autotuner chose for the plain warp solve, per lane
+ * layout (v_r <= 32, 64, 128, 256, 512, 1024): a candidate index (see
+ * wmd_solve_shape_name), -1 for the build-time default, -2 not tuned yet.
+ * Chosen on the first query of each layout after targets or embeddings are
+ * set (each candidate timed on the real panel, 4 updates), unless tuning is
+ * off (wmd_set_autotune).  No reference counterpart. */
+wmd_status wmd_solve_shape_choices(wmd_handle* h, int* shapes);
+const char* wmd_solve_shape_name(int shape);
+
 /* Launch-shape autotuner of the BF16 block solve (on by default): the first
  * solve of each panel width (and panel size class: within / beyond 64 MiB)
  * times every candidate shape on the handle's real data and keeps the

@@ -318,6 +318,24 @@ class Engine:
         for sources with 64 < v_r <= 512."""
         check(lib().wmd_set_solve_precision(self._h, {"fp32": 0, "bf16": 1}[prec]))
 
+    def set_batch_mode(self, stacked: bool = True, group_budget_gib: float = 32.0):
+        """Batched queries in stacked groups (a fixed number of launches per
+        group of same-width sources, one persistent solve over all their
+        (source, document) pairs) or source by source."""
+        check(lib().wmd_set_batch_mode(self._h, int(bool(stacked)),
+                                       int(group_budget_gib * (1 << 30))))
+
+    def solve_shape_choices(self) -> dict:
+        """{largest v_r of the lane layout: the warp solve's tuned shape}."""
+        a = (ctypes.c_int * 6)()
+        check(lib().wmd_solve_shape_choices(self._h, a))
+        return {32 << i: lib().wmd_solve_shape_name(v).decode()
+                for i, v in enumerate(a) if v != -2}
+
+    @property
+    def last_batch_groups(self) -> int:
+        return int(lib().wmd_last_batch_groups(self._h))
+
     def set_solve_order(self, order: str):
         """'document' (default: a document's scalings on chip for every pass)
         or 'word' (the reference's word-major traversal: each K row read once

@@ -124,6 +124,9 @@ struct wmd_handle {
   bool autotune = true;
   int forced_shape = -2;  // wmd_set_block_shape (-2: none)
   int blk_shape[8] = {-2, -2, -2, -2, -2, -2, -2, -2};  // -2: not tuned yet
+  // Launch shape of the plain warp solve per lane layout (v_r <= 32, 64, ...,
+  // 1024), tuned on this handle's target set; -2: not tuned yet.
+  int warp_shape[6] = {-2, -2, -2, -2, -2, -2};
   // Documents longer than the tensor-core solve's capacity, per panel width
   // (-1: not counted yet for this target set).
   int64_t tc_long[4][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
@@ -151,6 +154,14 @@ struct wmd_handle {
   // Word-major solve order (solve_word.cu): the target set as word-major CSR
   // (built on first use per target set) and the u / x state it streams.
   int solve_order = 0;  // 0 document-major, 1 word-major
+  // Stacked batch groups (batch.cu): on/off, device memory budget of one
+  // group's panels, their pools and tables, and the tuned launch shape of the
+  // stacked block solve per BF16 panel width.
+  bool stacked = true;
+  uint64_t group_budget = 32ull << 30;
+  DevBuf g_pool, g_pool16, g_vst, g_S, g_nS, g_S16, g_rowword, g_rowsrc, g_tiles, g_src;
+  int grp_shape[4] = {-2, -2, -2, -2};
+  int last_groups = 0;
   bool wm_ready = false;
   DevBuf wm_rp, wm_ent, wm_u, wm_x;
   // batched queries
@@ -292,6 +303,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
   h->e16_fmt = -1;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
   h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
@@ -365,6 +377,7 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   h->wm_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
   for (auto& row : h->tc_long)
     for (int64_t& x : row) x = -1;
   h->doc_len.resize(N);
@@ -489,6 +502,50 @@ int block_shape_for(wmd_handle* h, const void* K16, int ld16, float expo,
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   h->blk_shape[key] = bi;
+  return bi;
+}
+
+// Launch shape of the plain warp solve for sources of up to `cap` words,
+// cached per lane layout; when not yet known and the call may synchronise,
+// each candidate (warps per CTA x CTAs per SM) is timed on the real panel and
+// target set (4 updates, CUDA events) and the fastest is kept.  -1: the
+// build-time default (tuning off, inside a capture, or not a plain solve).
+int warp_shape_for(wmd_handle* h, const float* K, int ld, float expo, uint32_t cap,
+                   const SourceSel& sel, const Targets& t, const SolveCtl& ctl,
+                   double* out, bool can_sync) {
+  if (ctl.omega != 1.f || expo == 0.f) return -1;
+  int k = 0;
+  while (k < 5 && (32u << k) < cap) ++k;
+  if (h->warp_shape[k] != -2) return h->warp_shape[k];
+  if (!h->autotune || !can_sync) return -1;
+  SolveCtl c2 = ctl;
+  c2.max_iter = 4;
+  c2.tol = 0.f;
+  c2.iters = nullptr;
+  c2.u0 = nullptr;
+  c2.mrow = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    if (a) cudaEventDestroy(a);
+    return -1;
+  }
+  float best = 1e30f;
+  int bi = -1;
+  for (int sh = 0; sh < solve_shape_count(); ++sh) {
+    if (launch_solve(K, nullptr, ld, expo, cap, sel, t, c2, out, h->stream, sh) < 0) continue;
+    cudaEventRecord(a, h->stream);
+    launch_solve(K, nullptr, ld, expo, cap, sel, t, c2, out, h->stream, sh);
+    cudaEventRecord(b, h->stream);
+    float ms = 0.f;
+    if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess &&
+        ms < best) {
+      best = ms;
+      bi = sh;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  h->warp_shape[k] = bi;
   return bi;
 }
 
@@ -719,8 +776,10 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
       if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "block solve unavailable");
       n += ls;
     } else {
+      const int shape = KMp ? -1 : warp_shape_for(h, h->K.as<float>(), ld, expo, cap, sel,
+                                                  t, ctl, out_dev, !capturing);
       n += launch_solve(h->K.as<float>(), KMp, ld, expo, cap, sel, t, ctl,
-                        out_dev, h->stream);
+                        out_dev, h->stream, shape);
     }
     if (mrow) {  // documents the row-scaled FP32 panel cannot carry, in FP64
       const int le = launch_exact_f64(h->E32.as<float>(), d, sel, t, expo, ctl, mdl,
@@ -869,6 +928,214 @@ wmd_status topk_device(wmd_handle* h, const double* scores_dev, uint64_t n,
 // already applied.  All sources are uploaded once; per source a gather, the
 // cost panel, the near-pair fix-up and the solve run back to back on the
 // handle's stream, re-using the single-source working buffers.
+// Stacked batch: the sources of one width class run as groups whose panels
+// fit h->group_budget, each group in a fixed number of launches (batch.cu):
+// gather of the stacked source rows, one cost-panel launch writing every
+// source's panel, the near-pair fix-up, (BF16 classes) the BF16 panels, and
+// one persistent solve over all (source, document) pairs.  ids32 / rinv /
+// vrs are the validated host arrays of query_batch, already uploaded into
+// b_ids / b_rinv / b_vr.  form: the tensor-core cost-panel form.
+wmd_status query_batch_stacked(wmd_handle* h, uint64_t S, const uint64_t* src_ptr,
+                               const std::vector<uint32_t>& ids32,
+                               const std::vector<uint32_t>& vrs, int form, float expo,
+                               int max_iter, int* launches_out) {
+  const uint64_t V = h->V, d = h->d, N = h->N, nnz = h->nnz;
+  const bool bf16p = h->prec == WMD_SOLVE_BF16;
+  const bool x3 = form == TC_TF32X3;
+  const bool tcm = !x3;
+  const int dp = tc_padded_width(d);
+  const bool relax = h->tol > 0.f && h->omega != 1.f;
+  // width class: a BF16 panel width (block solve) or a lane layout (warp solve)
+  auto ld16_of = [&](uint32_t vr) { return bf16p ? block_panel_width(vr) : 0; };
+  auto cls_of = [&](uint32_t vr) -> int {
+    const int l16 = ld16_of(vr);
+    if (l16) return 100 + l16 / 128;
+    int lpw = 1;
+    while (32 * lpw < (int)std::max<uint32_t>(vr, 1)) lpw <<= 1;
+    return lpw;
+  };
+  std::vector<int> classes;
+  for (uint64_t s = 0; s < S; ++s) {
+    const int c = cls_of(vrs[s]);
+    if (std::find(classes.begin(), classes.end(), c) == classes.end()) classes.push_back(c);
+  }
+  std::sort(classes.begin(), classes.end());
+  Targets t;
+  t.col_ptr = h->col_ptr.as<int64_t>();
+  t.ent = h->ent.as<uint2>();
+  t.order = h->order.as<int32_t>();
+  t.N = (int64_t)N;
+  t.nnz = (int64_t)nnz;
+  int launches = 0, groups = 0;
+  for (int cls : classes) {
+    std::vector<uint64_t> members;
+    for (uint64_t s = 0; s < S; ++s)
+      if (cls_of(vrs[s]) == cls) members.push_back(s);
+    const int l16 = cls > 100 ? 128 * (cls - 100) : 0;
+    size_t m0 = 0;
+    while (m0 < members.size()) {
+      // the next group: as many members as the budget holds (at least one)
+      size_t m1 = m0;
+      uint64_t bytes = 0;
+      while (m1 < members.size()) {
+        const uint32_t vr = vrs[members[m1]];
+        const uint64_t ld = ((vr ? vr : 1) + 3u) & ~3u;
+        const uint64_t b = V * ld * 4 + (l16 ? V * (uint64_t)l16 * 2 : 0) +
+                           (relax ? std::max<uint64_t>(nnz, 1) * 4 : 0);
+        if (m1 > m0 && bytes + b > h->group_budget) break;
+        bytes += b;
+        ++m1;
+      }
+      const int ng = (int)(m1 - m0);
+      uint32_t vmax = 1;
+      for (size_t m = m0; m < m1; ++m) vmax = std::max(vmax, vrs[members[m]]);
+      const int NT = x3 ? tc_tile_n_x3(vmax, d) : tc_tile_n(vmax, d);
+      if (NT == 0) return fail(WMD_ERR_UNSUPPORTED, "cost panel cannot tile this width");
+      // host tables: stacked rows, tiles, per-source descriptors
+      std::vector<int32_t> rowword, rowsrc;
+      std::vector<int4> tiles;
+      std::vector<GroupSrc> src(ng);
+      uint64_t off32 = 0, off16 = 0, offv = 0;
+      for (int k = 0; k < ng; ++k) {
+        const uint64_t s = members[m0 + k];
+        const uint32_t vr = vrs[s];
+        const int ld = (int)(((vr ? vr : 1) + 3u) & ~3u);
+        const int nt = (ld + NT - 1) / NT;
+        GroupSrc& g = src[k];
+        g.vr = (int)vr;
+        g.ld = ld;
+        g.row0 = (int)rowword.size();
+        g.rinv = h->b_rinv.as<float>() + src_ptr[s];
+        g.vr_dev = h->b_vr.as<uint32_t>() + s;
+        g.out = h->b_out.as<double>() + s * N;
+        g.iters = h->b_iters.as<int>() + s * N;
+        g.K = reinterpret_cast<float*>(off32);    // offsets, rebased below
+        g.K16 = l16 ? reinterpret_cast<void*>(off16) : nullptr;
+        g.vstate = relax ? reinterpret_cast<float*>(offv) : nullptr;
+        off32 += V * (uint64_t)ld * 4;
+        off16 += l16 ? V * (uint64_t)l16 * 2 : 0;
+        offv += relax ? std::max<uint64_t>(nnz, 1) * 4 : 0;
+        for (int i = 0; i < nt * NT; ++i) {
+          rowword.push_back(i < (int)vr ? (int32_t)ids32[src_ptr[s] + i] : -1);
+          rowsrc.push_back(k);
+        }
+        for (int i = 0; i < nt; ++i) tiles.push_back(make_int4(k, g.row0 + i * NT, i * NT, 0));
+      }
+      const int rows = (int)rowword.size();
+      CK(h->g_pool.ensure(std::max<uint64_t>(off32, 256)));
+      if (l16) CK(h->g_pool16.ensure(std::max<uint64_t>(off16, 256)));
+      if (relax) CK(h->g_vst.ensure(std::max<uint64_t>(offv, 256)));
+      for (GroupSrc& g : src) {
+        g.K = reinterpret_cast<float*>(h->g_pool.as<unsigned char>() +
+                                       reinterpret_cast<uintptr_t>(g.K));
+        if (l16)
+          g.K16 = h->g_pool16.as<unsigned char>() + reinterpret_cast<uintptr_t>(g.K16);
+        if (relax)
+          g.vstate = reinterpret_cast<float*>(h->g_vst.as<unsigned char>() +
+                                              reinterpret_cast<uintptr_t>(g.vstate));
+      }
+      CK(h->g_S.ensure((size_t)rows * d * 4));
+      CK(h->g_nS.ensure((size_t)rows * 4));
+      if (tcm) CK(h->g_S16.ensure((size_t)rows * dp * 2));
+      CK(h->g_rowword.ensure((size_t)rows * 4));
+      CK(h->g_rowsrc.ensure((size_t)rows * 4));
+      CK(h->g_tiles.ensure(tiles.size() * sizeof(int4)));
+      CK(h->g_src.ensure(src.size() * sizeof(GroupSrc)));
+      const unsigned near_cap =
+          (unsigned)std::min<uint64_t>((uint64_t)V * rows, (uint64_t)rows * 64 + 4096);
+      CK(h->near_pairs.ensure((size_t)near_cap * sizeof(uint2)));
+      CK(h->near_count.ensure(sizeof(unsigned)));
+      // pageable sources: each copy has been staged when the call returns
+      CK(cudaMemcpyAsync(h->g_rowword.p, rowword.data(), (size_t)rows * 4,
+                         cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->g_rowsrc.p, rowsrc.data(), (size_t)rows * 4,
+                         cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->g_tiles.p, tiles.data(), tiles.size() * sizeof(int4),
+                         cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->g_src.p, src.data(), src.size() * sizeof(GroupSrc),
+                         cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemsetAsync(h->near_count.p, 0, sizeof(unsigned), h->stream));
+      launches += launch_group_gather(h->g_rowword.as<int32_t>(), rows, h->E32.as<float>(),
+                                      h->nE.as<float>(), d, h->g_S.as<float>(),
+                                      h->g_nS.as<float>(), tcm ? h->E16.p : nullptr,
+                                      tcm ? h->g_S16.p : nullptr, dp, h->sms, h->stream);
+      SourceSel sel;
+      sel.S = h->g_S.as<float>();
+      sel.nS = h->g_nS.as<float>();
+      sel.cap = (uint32_t)rows;
+      NearList near;
+      near.pairs = h->near_pairs.as<uint2>();
+      near.count = h->near_count.as<unsigned>();
+      near.cap = near_cap;
+      near.E32 = h->E32.as<float>();
+      near.S32 = sel.S;
+      near.d = (int)d;
+      StackedPanels sp;
+      sp.tiles = h->g_tiles.as<int4>();
+      sp.src = h->g_src.as<GroupSrc>();
+      sp.ntiles = (int)tiles.size();
+      sp.nt = NT;
+      const int lc = launch_cdist_tc(form, h->E16.p, h->g_S16.p, h->E32.as<float>(),
+                                     h->nE.as<float>(), V, d, sel, expo, nullptr, nullptr,
+                                     0, near, h->err_dev.as<unsigned>(), h->sms, h->stream,
+                                     nullptr, &sp);
+      if (lc < 0) return fail(WMD_ERR_UNSUPPORTED, "stacked cost panel unavailable");
+      launches += lc;
+      launches += launch_near_fixup_group(near, expo, h->g_rowsrc.as<int32_t>(),
+                                          sp.src, ng, V, h->nE.as<float>(),
+                                          h->g_nS.as<float>(), h->sms, h->stream);
+      SolveCtl ctl;
+      ctl.max_iter = max_iter;
+      ctl.tol = h->tol;
+      ctl.omega = relax ? h->omega : 1.f;
+      ctl.vstate = nullptr;  // per source, in src[]
+      int ls;
+      if (l16) {
+        launches += launch_panel_to_bf16_group(sp.src, ng, V, l16, h->sms, h->stream);
+        int& shp = h->grp_shape[l16 / 128 - 1];
+        if (shp == -2) {
+          // autotune the stacked block solve's launch shape on this group
+          // (4 updates of every pair per candidate, CUDA events)
+          SolveCtl c2 = ctl;
+          c2.max_iter = 4;
+          c2.tol = 0.f;
+          c2.omega = 1.f;
+          cudaEvent_t a = nullptr, b = nullptr;
+          CK(cudaEventCreate(&a));
+          CK(cudaEventCreate(&b));
+          float best = 1e30f;
+          int bi = 0;
+          for (int sh = 0; sh < 3; ++sh) {
+            if (launch_block_group(sp.src, ng, l16, expo, t, c2, sh, h->stream) < 0) continue;
+            cudaEventRecord(a, h->stream);
+            launch_block_group(sp.src, ng, l16, expo, t, c2, sh, h->stream);
+            cudaEventRecord(b, h->stream);
+            float ms = 0.f;
+            if (cudaEventSynchronize(b) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, a, b) == cudaSuccess && ms < best) {
+              best = ms;
+              bi = sh;
+            }
+          }
+          cudaEventDestroy(a);
+          cudaEventDestroy(b);
+          shp = bi;
+        }
+        ls = launch_block_group(sp.src, ng, l16, expo, t, ctl, shp, h->stream);
+      } else {
+        ls = launch_solve_group(vmax, sp.src, ng, expo, t, ctl, h->stream);
+      }
+      if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "stacked solve unavailable");
+      launches += ls;
+      ++groups;
+      m0 = m1;
+    }
+  }
+  h->last_groups = groups;
+  *launches_out = launches;
+  return WMD_OK;
+}
+
 wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
                        const uint64_t* src_ids, const double* src_w, uint64_t S,
                        float expo, int max_iter, double* wmd_out, int* iters_out) {
@@ -1002,6 +1269,25 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   t.nnz = (int64_t)h->nnz;
   if (h->timing)
     for (int i = 0; i < 3; ++i) CK(cudaEventRecord(h->ev[i], h->stream));
+  // Stacked groups (batch.cu): several sources, tensor-core cost panel, cold
+  // start, lambda != 0, panels within FP32 range.
+  if (h->stacked && S > 1 && expo != 0.f && !scaled && !ws && (tcm || x3)) {
+    int lg = 0;
+    wmd_status sg = query_batch_stacked(h, S, src_ptr, ids32, vrs,
+                                        x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16, expo,
+                                        max_iter, &lg);
+    if (sg) return sg;
+    if (h->timing) CK(cudaEventRecord(h->ev[3], h->stream));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(wmd_out, h->b_out.p, S * N * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
+    if (iters_out)
+      CK(cudaMemcpyAsync(iters_out, h->b_iters.p, S * N * sizeof(int),
+                         cudaMemcpyDeviceToHost, h->stream));
+    h->last_launches = launches + lg;
+    return finish(h);
+  }
+  h->last_groups = 0;
   if (overlap) {  // slot 1 starts after the uploads above
     CK(cudaEventRecord(h->join[0], h->stream));
     CK(cudaStreamWaitEvent(h->stream2, h->join[0], 0));
@@ -1209,6 +1495,7 @@ wmd_status set_embeddings_needed(wmd_handle* h, const double* vecs_mapped,
   h->e16_fmt = -1;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
   h->graph_epoch++;
   h->last_launches = launches;
   return WMD_OK;
@@ -1448,6 +1735,7 @@ wmd_status wmd_set_autotune(wmd_handle* h, int enable) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
   h->autotune = enable != 0;
   for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
   h->graph_epoch++;
   return WMD_OK;
 }
@@ -1468,6 +1756,25 @@ wmd_status wmd_autotune_choices(wmd_handle* h, int* shapes) {
 }
 
 const char* wmd_block_shape_name(int shape) { return block_shape_name(shape); }
+
+wmd_status wmd_set_batch_mode(wmd_handle* h, int stacked, uint64_t group_budget_bytes) {
+  if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
+  if (group_budget_bytes < (64ull << 20))
+    return fail(WMD_ERR_INVALID_ARG, "group budget below 64 MiB");
+  h->stacked = stacked != 0;
+  h->group_budget = group_budget_bytes;
+  return WMD_OK;
+}
+
+int wmd_last_batch_groups(wmd_handle* h) { return h ? h->last_groups : 0; }
+
+wmd_status wmd_solve_shape_choices(wmd_handle* h, int* shapes) {
+  if (!h || !shapes) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  for (int i = 0; i < 6; ++i) shapes[i] = h->warp_shape[i];
+  return WMD_OK;
+}
+
+const char* wmd_solve_shape_name(int shape) { return solve_shape_name(shape); }
 
 wmd_status wmd_set_solve_order(wmd_handle* h, int order) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
@@ -2152,6 +2459,7 @@ wmd_status wmd_set_targets_edges(wmd_handle* h, const uint64_t* words,
   h->wm_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
   for (auto& row : h->tc_long)
     for (int64_t& x : row) x = -1;
   h->doc_len.resize(N);

@@ -88,6 +88,11 @@ struct Params {
   float* KM;          // [V][ld] or null (then K*M is not stored)
   NearList near;      // cancellation-prone pairs for the exact fix-up pass
   float* mrow;        // row-scaled form: [V] row minima of M (else null)
+  // Stacked batch group (null: one source): N-tile blockIdx.y covers rows
+  // [tiles[y].y, + NT) of the stacked source rows, which are columns
+  // [tiles[y].z, + NT) of source tiles[y].x's panel (grp[]).
+  const int4* tiles;
+  const GroupSrc* grp;
   unsigned* err;
   uint64_t V;
   int d, ld, NT, KT, tmem_cols, stages;
@@ -169,8 +174,23 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
   float* nS_s = reinterpret_cast<float*>(tmem_slot + 4);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.y * p.NT;
-  const int vr = (int)*p.vr;
+  // This CTA's N-tile: its first stacked source row (TMA, norms, near-pair
+  // ids), its first panel column, and the panel it writes.
+  int n0 = blockIdx.y * p.NT, col0 = n0, vr, ldk = p.ld;
+  float* Kt = p.K;
+  float* mrowt = p.mrow;
+  if (p.tiles) {
+    const int4 tl = p.tiles[blockIdx.y];
+    const GroupSrc& gs = p.grp[tl.x];
+    n0 = tl.y;
+    col0 = tl.z;
+    vr = gs.vr;
+    ldk = gs.ld;
+    Kt = gs.K;
+    mrowt = gs.mrow;
+  } else {
+    vr = (int)*p.vr;
+  }
   const int ntiles = (int)((p.V + BM - 1) / BM);
 
   if (threadIdx.x == 0) {
@@ -198,15 +218,14 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   for (int c = threadIdx.x; c < p.NT; c += blockDim.x) {
-    const int i = n0 + c;
-    nS_s[c] = i < vr ? p.nS[i] : 0.f;
+    nS_s[c] = col0 + c < vr ? p.nS[n0 + c] : 0.f;
   }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (n0 < vr) {
+  if (col0 < vr) {
     if (warp == 0) {
       if (lane == 0) {
         // ---- TMA producer ----
@@ -369,8 +388,8 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
           // columns past v_r are zeroed last.
           float kv[16], kmv[16];
           unsigned nearmask = 0;
-          const int nval = vr - (n0 + c0);  // valid columns of this chunk
-          if (p.mrow) {
+          const int nval = vr - (col0 + c0);  // valid columns of this chunk
+          if (mrowt) {
             // Row-scaled form: M now (and the row minimum), K' after the
             // near-pair fix-up (panel_rescale.cu).
 #pragma unroll
@@ -409,22 +428,22 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             nearmask &= nearmask - 1u;
             near_pair(p.near, w, n0 + c0 + j);
           }
-          float* krow = p.K + w * (uint64_t)p.ld;
-          float* kmrow = p.KM + w * (uint64_t)p.ld;
+          float* krow = Kt + w * (uint64_t)ldk;
+          float* kmrow = p.KM + w * (uint64_t)ldk;
 #pragma unroll
           for (int j4 = 0; j4 < 4; ++j4) {
-            const int c = n0 + c0 + 4 * j4;
-            if (c < p.ld) {
+            const int c = col0 + c0 + 4 * j4;
+            if (c < ldk) {
               *reinterpret_cast<float4*>(krow + c) = make_float4(
                   kv[4 * j4], kv[4 * j4 + 1], kv[4 * j4 + 2], kv[4 * j4 + 3]);
-              if (p.KM && !p.mrow)
+              if (p.KM && !mrowt)
                 *reinterpret_cast<float4*>(kmrow + c) = make_float4(
                     kmv[4 * j4], kmv[4 * j4 + 1], kmv[4 * j4 + 2], kmv[4 * j4 + 3]);
             }
           }
         }
-        if (p.mrow && wok && mmin < __int_as_float(0x7f7f7f7f))
-          atomicMin(reinterpret_cast<int*>(p.mrow + w), __float_as_int(mmin));
+        if (mrowt && wok && mmin < __int_as_float(0x7f7f7f7f))
+          atomicMin(reinterpret_cast<int*>(mrowt + w), __float_as_int(mmin));
         fence_before();
         mbar_arrive(&acce[b]);
       }
@@ -435,8 +454,8 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
       const uint64_t w = (uint64_t)tile * BM + quarter * 32 + lane;
       if (w >= p.V) continue;
-      for (int c = n0; c < n0 + p.NT && c < p.ld; c += 4) {
-        *reinterpret_cast<float4*>(p.K + w * (uint64_t)p.ld + c) = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int c = col0; c < col0 + p.NT && c < ldk; c += 4) {
+        *reinterpret_cast<float4*>(Kt + w * (uint64_t)ldk + c) = make_float4(0.f, 0.f, 0.f, 0.f);
         if (p.KM)
           *reinterpret_cast<float4*>(p.KM + w * (uint64_t)p.ld + c) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
@@ -571,13 +590,14 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
                     const NearList& near, unsigned* err, int num_sms,
-                    cudaStream_t st, float* mrow) {
+                    cudaStream_t st, float* mrow, const StackedPanels* grp) {
   const bool x3 = form == TC_TF32X3;
+  // stacked group: s.cap is the number of stacked source rows
   const uint64_t rows_b = s.cap ? s.cap : 1;
   int NT, KT;
   CUtensorMap tmA, tmB;
   if (x3) {
-    NT = tc_tile_n_x3(s.cap, d);
+    NT = grp ? grp->nt : tc_tile_n_x3(s.cap, d);
     if (NT == 0) return -1;
     KT = (int)((d + 31) / 32);
     // FP32 rows in place, 32-float (128-byte) chunks; the last chunk's
@@ -589,7 +609,7 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
       return -1;
   } else {
     const int dp = tc_padded_width(d);
-    NT = tc_tile_n(s.cap, d);
+    NT = grp ? grp->nt : tc_tile_n(s.cap, d);
     if (NT == 0) return -1;
     KT = (dp + tc::BK - 1) / tc::BK;
     const CUtensorMapDataType dt = form == TC_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
@@ -599,8 +619,10 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
     if (!make_map(&tmB, S16, dt, 2, (uint64_t)dp, rows_b, tc::BK, (uint32_t)NT))
       return -1;
   }
-  const int ntn = (ld + NT - 1) / NT;
+  const int ntn = grp ? grp->ntiles : (ld + NT - 1) / NT;
   tc::Params p;
+  p.tiles = grp ? grp->tiles : nullptr;
+  p.grp = grp ? grp->src : nullptr;
   p.E32 = E32;
   p.nE = nE;
   p.S32 = s.S;

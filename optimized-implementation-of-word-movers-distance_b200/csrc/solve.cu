@@ -147,8 +147,15 @@ struct SolveShape {
   }
 };
 
-template <int LPW, bool FROM_KM, bool RLX>
-__global__ void __launch_bounds__(SolveCfg<LPW>::kWarps * 32, SolveCfg<LPW>::kCtas)
+// GRP: the stacked form of a batch (batch.cu): the work items are (source,
+// document) pairs, source-major, over `nsrc` sources whose panel, weights and
+// outputs come from grp[]; the per-source arguments below are then replaced
+// item by item.
+// kW, kC: warps per CTA and CTAs per SM of this instantiation (the
+// build-time default shape, or an autotuner candidate).
+template <int LPW, bool FROM_KM, bool RLX, bool GRP, int kW = SolveCfg<LPW>::kWarps,
+          int kC = SolveCfg<LPW>::kCtas>
+__global__ void __launch_bounds__(kW * 32, kC)
 solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              float expo, const uint32_t* __restrict__ vr_dev,
              const float* __restrict__ rinv,
@@ -158,7 +165,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
              float tol, int* __restrict__ iters_out, int srounds,
              const float* __restrict__ u0, int64_t ldu, float omega,
              float* __restrict__ vstate, const float* __restrict__ mrow,
-             double* __restrict__ out) {
+             double* __restrict__ out, const GroupSrc* __restrict__ grp, int nsrc) {
   using Sh = SolveShape<LPW>;
   constexpr int WPS = Sh::WPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -171,8 +178,8 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   float* red = reinterpret_cast<float*>(wbase + Sh::staged_bytes(srounds) +
                                         Sh::entries_bytes(srounds));
   float* ubuf = red + 32 * 32;
-  const int vr = (int)*vr_dev;
-  const int ldc = ld >> 2;  // float4 chunks per global panel row
+  int vr = GRP ? 0 : (int)*vr_dev;
+  int ldc = ld >> 2;  // float4 chunks per global panel row
   // Staged row s holds logical chunk 8q'+t at 8q' + (t ^ ((s*LPW + q') & 7)).
   // For the lane that reads it s*LPW + q = 32*round + lane, so the key is
   // lane & 7: constant per lane, and the 8 lanes of a shared-memory phase hit
@@ -186,16 +193,22 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   const int own = kPairSum ? 2 * (lane & 15) + (lane >> 4) : lane;
   float rv[LPW], rw[LPW];  // 1/r_i and r_i
   unsigned dmask = 0;
+  auto set_dims = [&]() {
+    dmask = 0;
 #pragma unroll
-  for (int qq = 0; qq < LPW; ++qq) {
-    const int D = 32 * qq + own;
-    const bool ok = D < vr;
-    rv[qq] = ok ? rinv[D] : 0.f;
-    rw[qq] = ok ? __frcp_rn(rv[qq]) : 0.f;
-    dmask |= ok ? (1u << qq) : 0u;
-  }
+    for (int qq = 0; qq < LPW; ++qq) {
+      const int D = 32 * qq + own;
+      const bool ok = D < vr;
+      rv[qq] = ok ? rinv[D] : 0.f;
+      rw[qq] = ok ? __frcp_rn(rv[qq]) : 0.f;
+      dmask |= ok ? (1u << qq) : 0u;
+    }
+  };
+  if constexpr (!GRP) set_dims();
+  int cur_src = -1;
+  const int64_t NI = GRP ? N * (int64_t)nsrc : N;  // work items
 
-  constexpr int kWarps = SolveCfg<LPW>::kWarps;
+  constexpr int kWarps = kW;
   const int64_t total_warps = (int64_t)gridDim.x * kWarps;
   // Persistent warps over the documents in decreasing-length order, in
   // "snake" order: in lap p over the grid, warp w takes position
@@ -203,29 +216,51 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   // of the longest documents of a lap draws one of the shortest of the
   // next.  A plain stride hands warp 0 the longest document of every lap
   // (about 22 % above the mean load at the single-source workload).
-  // Positions grow strictly with p, so the loop ends at the first >= N.
+  // Positions grow strictly with p, so the loop ends at the first >= NI.
   const int64_t wid = (int64_t)blockIdx.x * kWarps + warp;
   auto position = [&](int64_t p) -> int64_t {
     return p * total_warps + ((p & 1) ? total_warps - 1 - wid : wid);
   };
   int64_t lap = 0;
   int64_t idx = position(0);
+  // Item -> (source, position in the document order).
+  auto doc_of = [&](int64_t it) -> int64_t {
+    const int64_t pos = GRP ? it % N : it;
+    return order ? (int64_t)__ldg(&order[pos]) : pos;
+  };
   // Pointers of the current document; the next one's are prefetched while
   // this one is processed.
   int64_t j = 0, b = 0;
   int n = 0;
-  if (idx < N) {
-    j = order ? (int64_t)order[idx] : idx;
+  if (idx < NI) {
+    j = doc_of(idx);
     b = col_ptr[j];
     n = (int)(col_ptr[j + 1] - b);
   }
-  for (; idx < N; idx = position(++lap)) {
+  for (; idx < NI; idx = position(++lap)) {
+    if constexpr (GRP) {
+      const int src = (int)(idx / N);
+      if (src != cur_src) {  // this source's panel, weights and outputs
+        const GroupSrc& gs = grp[src];
+        K = gs.K;
+        ld = gs.ld;
+        ldc = ld >> 2;
+        vr = gs.vr;
+        rinv = gs.rinv;
+        iters_out = gs.iters;
+        vstate = gs.vstate;
+        mrow = gs.mrow;
+        out = gs.out;
+        set_dims();
+        cur_src = src;
+      }
+    }
     RelaxGuard rg;  // over-relaxation of this document (RLX instantiations)
     rg.init(omega);
     float resv = 0.f;  // this lane's c-side residual of the current pass
     const int64_t nidx = position(lap + 1);
     int64_t jn = 0;
-    if (nidx < N) jn = order ? (int64_t)__ldg(&order[nidx]) : nidx;
+    if (nidx < NI) jn = doc_of(nidx);
     const int rounds = (n + WPS - 1) / WPS;
     constexpr int RR = Sh::RR;
     const int rr = rounds < RR ? rounds : RR;                   // in registers
@@ -275,7 +310,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     // Next document's pointers (the order[] load has landed by now).
     int64_t bn = 0;
     int nn = 0;
-    if (nidx < N) {
+    if (nidx < NI) {
       bn = __ldg(&col_ptr[jn]);
       nn = (int)(__ldg(&col_ptr[jn + 1]) - bn);
     }
@@ -639,14 +674,16 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   }
 }
 
-template <int LPW, bool FROM_KM, bool RLX>
+template <int LPW, bool FROM_KM, bool RLX, bool GRP = false,
+          int kW = SolveCfg<LPW>::kWarps, int kC = SolveCfg<LPW>::kCtas>
 static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
                           const SourceSel& s, const Targets& t,
-                          const SolveCtl& ctl, double* out, cudaStream_t st) {
+                          const SolveCtl& ctl, double* out, cudaStream_t st,
+                          const GroupSrc* grp = nullptr, int nsrc = 0) {
   using Sh = SolveShape<LPW>;
   constexpr int kMaxDev = 64;
-  constexpr int kBlocksPerSm = SolveCfg<LPW>::kCtas;
-  constexpr int kWarps = SolveCfg<LPW>::kWarps;
+  constexpr int kBlocksPerSm = kC;
+  constexpr int kWarps = kW;
   constexpr size_t kSmemPerSm = 227 * 1024;
   static int sms_cache[kMaxDev] = {0};
   static int srounds_cache[kMaxDev] = {0};
@@ -659,7 +696,7 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
     const size_t per_round = Sh::staged_bytes(1) + (size_t)Sh::WPS * 8;
     int sr = per_warp > fixed ? (int)((per_warp - fixed) / per_round) : 0;
     while (sr > 0 && Sh::warp_bytes(sr) > per_warp) --sr;
-    cudaFuncSetAttribute(solve_kernel<LPW, FROM_KM, RLX>,
+    cudaFuncSetAttribute(solve_kernel<LPW, FROM_KM, RLX, GRP, kW, kC>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(kWarps * Sh::warp_bytes(sr)));
     int sms = 0;
@@ -669,15 +706,44 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   }
   const int sr = srounds_cache[dev];
   const size_t smem = (size_t)kWarps * Sh::warp_bytes(sr);
-  int64_t want = (t.N + kWarps - 1) / kWarps;
+  const int64_t items = GRP ? t.N * (int64_t)nsrc : t.N;
+  int64_t want = (items + kWarps - 1) / kWarps;
   int64_t grid = (int64_t)sms_cache[dev] * kBlocksPerSm;
   if (grid > want) grid = want;
   if (grid < 1) grid = 1;
-  solve_kernel<LPW, FROM_KM, RLX><<<(unsigned)grid, kWarps * 32, smem, st>>>(
+  solve_kernel<LPW, FROM_KM, RLX, GRP, kW, kC><<<(unsigned)grid, kWarps * 32, smem, st>>>(
       K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
       ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, ctl.vstate,
-      ctl.mrow, out);
+      ctl.mrow, out, grp, nsrc);
   return 1;
+}
+
+// Stacked batch group: one persistent launch over every (source, document)
+// pair of `nsrc` sources of one lane-layout class (v_r <= vr_max), source-
+// major so that the grid works on one or two sources' panels at a time.
+template <int LPW>
+static int launch_group_t(const GroupSrc* grp, int nsrc, float expo, const Targets& t,
+                          const SolveCtl& ctl, cudaStream_t st) {
+  SourceSel none;
+  if (ctl.omega != 1.f)
+    return launch_solve_t<LPW, false, true, true>(nullptr, nullptr, 4, expo, none, t, ctl,
+                                                  nullptr, st, grp, nsrc);
+  return launch_solve_t<LPW, false, false, true>(nullptr, nullptr, 4, expo, none, t, ctl,
+                                                 nullptr, st, grp, nsrc);
+}
+
+int launch_solve_group(uint32_t vr_max, const GroupSrc* grp, int nsrc, float expo,
+                       const Targets& t, const SolveCtl& ctl, cudaStream_t st) {
+  if (t.N <= 0 || nsrc <= 0) return 0;
+  SolveCtl c = ctl;
+  c.u0 = nullptr;  // cold start only in the stacked form
+  if (vr_max <= 32) return launch_group_t<1>(grp, nsrc, expo, t, c, st);
+  if (vr_max <= 64) return launch_group_t<2>(grp, nsrc, expo, t, c, st);
+  if (vr_max <= 128) return launch_group_t<4>(grp, nsrc, expo, t, c, st);
+  if (vr_max <= 256) return launch_group_t<8>(grp, nsrc, expo, t, c, st);
+  if (vr_max <= 512) return launch_group_t<16>(grp, nsrc, expo, t, c, st);
+  if (vr_max <= 1024) return launch_group_t<32>(grp, nsrc, expo, t, c, st);
+  return -1;
 }
 
 template <bool FROM_KM, bool RLX>
@@ -693,10 +759,43 @@ static int dispatch_solve(const float* K, const float* KM, int ld, float expo,
   return -1;
 }
 
+// Autotuner candidates of the plain (unrelaxed, lambda != 0) warp solve:
+// warps per CTA x CTAs per SM at the same eight warps per SM.
+int solve_shape_count() { return 3; }
+const char* solve_shape_name(int shape) {
+  switch (shape) {
+    case 0: return "1 warp x 8 CTAs/SM";
+    case 1: return "2 warps x 4 CTAs/SM";
+    case 2: return "4 warps x 2 CTAs/SM";
+  }
+  return "build-time default";
+}
+
+template <int LPW>
+static int launch_plain_shape(const float* K, int ld, float expo, const SourceSel& s,
+                              const Targets& t, const SolveCtl& c, double* out,
+                              cudaStream_t st, int shape) {
+  switch (shape) {
+    case 0: return launch_solve_t<LPW, false, false, false, 1, 8>(K, nullptr, ld, expo, s, t, c, out, st);
+    case 1: return launch_solve_t<LPW, false, false, false, 2, 4>(K, nullptr, ld, expo, s, t, c, out, st);
+    case 2: return launch_solve_t<LPW, false, false, false, 4, 2>(K, nullptr, ld, expo, s, t, c, out, st);
+  }
+  return launch_solve_t<LPW, false, false>(K, nullptr, ld, expo, s, t, c, out, st);
+}
+
 int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
-                 const SolveCtl& ctl, double* out, cudaStream_t st) {
+                 const SolveCtl& ctl, double* out, cudaStream_t st, int shape) {
   if (t.N <= 0) return 0;
+  if (shape >= 0 && !KM && ctl.omega == 1.f) {
+    if (vr_cap <= 32) return launch_plain_shape<1>(K, ld, expo, s, t, ctl, out, st, shape);
+    if (vr_cap <= 64) return launch_plain_shape<2>(K, ld, expo, s, t, ctl, out, st, shape);
+    if (vr_cap <= 128) return launch_plain_shape<4>(K, ld, expo, s, t, ctl, out, st, shape);
+    if (vr_cap <= 256) return launch_plain_shape<8>(K, ld, expo, s, t, ctl, out, st, shape);
+    if (vr_cap <= 512) return launch_plain_shape<16>(K, ld, expo, s, t, ctl, out, st, shape);
+    if (vr_cap <= 1024) return launch_plain_shape<32>(K, ld, expo, s, t, ctl, out, st, shape);
+    return -1;
+  }
   // lambda = 0 (KM read from a panel: K = 1 everywhere) runs unrelaxed.
   if (KM)
     return dispatch_solve<true, false>(K, KM, ld, expo, vr_cap, s, t, ctl, out, st);

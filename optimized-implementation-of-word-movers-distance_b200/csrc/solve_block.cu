@@ -87,7 +87,9 @@ struct BlockShape {
   }
 };
 
-template <int NQ, int kBW, int kCPS, bool RLX>
+// GRP: stacked batch group (batch.cu): work items are (source, document)
+// pairs, source-major, the per-source arguments taken from grp[] item by item.
+template <int NQ, int kBW, int kCPS, bool RLX, bool GRP = false>
 __global__ void __launch_bounds__(kBW * 32, kCPS)
 solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                    const uint32_t* __restrict__ vr_dev,
@@ -98,7 +100,8 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
                    float tol, int* __restrict__ iters_out,
                    const float* __restrict__ u0, int64_t ldu, int max_rows,
                    float omega, float* __restrict__ vstate,
-                   const float* __restrict__ mrow, double* __restrict__ out) {
+                   const float* __restrict__ mrow, double* __restrict__ out,
+                   const GroupSrc* __restrict__ grp = nullptr, int nsrc = 0) {
   using Sh = BlockShape<NQ, kBW>;
   constexpr int kBT = kBW * 32;
   constexpr int RL = Sh::RL;
@@ -114,18 +117,39 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
   double* red = reinterpret_cast<double*>(ubufB + RL);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool lo = lane < 16;
-  const int vr = (int)*vr_dev;
+  int vr = GRP ? 0 : (int)*vr_dev;
 
   float rv[DPT], rw[DPT];  // 1/r_i and r_i of this thread's update dimensions
+  auto set_dims = [&]() {
 #pragma unroll
-  for (int i = 0; i < DPT; ++i) {
-    const int D = tid + i * kBT;
-    rv[i] = D < vr ? rinv[D] : 0.f;
-    rw[i] = D < vr ? __frcp_rn(rv[i]) : 0.f;
-  }
+    for (int i = 0; i < DPT; ++i) {
+      const int D = tid + i * kBT;
+      rv[i] = D < vr ? rinv[D] : 0.f;
+      rw[i] = D < vr ? __frcp_rn(rv[i]) : 0.f;
+    }
+  };
+  if constexpr (!GRP) set_dims();
+  int cur_src = -1;
+  const int64_t NI = GRP ? N * (int64_t)nsrc : N;  // work items
 
-  for (int64_t idx = blockIdx.x; idx < N; idx += gridDim.x) {
-    const int64_t j = order ? (int64_t)order[idx] : idx;
+  for (int64_t idx = blockIdx.x; idx < NI; idx += gridDim.x) {
+    if constexpr (GRP) {
+      const int src = (int)(idx / N);
+      if (src != cur_src) {  // this source's panel, weights and outputs
+        const GroupSrc& gs = grp[src];
+        K16 = static_cast<const uint2*>(gs.K16);
+        vr = gs.vr;
+        rinv = gs.rinv;
+        iters_out = gs.iters;
+        vstate = gs.vstate;
+        mrow = gs.mrow;
+        out = gs.out;
+        set_dims();
+        cur_src = src;
+      }
+    }
+    const int64_t pos = GRP ? idx % N : idx;
+    const int64_t j = order ? (int64_t)order[pos] : pos;
     const int64_t b = col_ptr[j];
     const int n = (int)(col_ptr[j + 1] - b);
     const int ns = n < max_rows ? n : max_rows;  // rows staged in shared memory
@@ -424,11 +448,12 @@ int launch_panel_to_bf16(const float* K, int ld, void* K16, int ld16, uint64_t V
   return 1;
 }
 
-template <int NQ, int kBW, int kCPS, bool RLX>
+template <int NQ, int kBW, int kCPS, bool RLX, bool GRP = false>
 static int launch_block_t(const void* K16, int ld16, float expo,
                           const SourceSel& s, const Targets& t,
                           const SolveCtl& ctl, const float* u0, int64_t ldu,
-                          double* out, cudaStream_t st) {
+                          double* out, cudaStream_t st,
+                          const GroupSrc* grp = nullptr, int nsrc = 0) {
   using Sh = BlockShape<NQ, kBW>;
   constexpr int kMaxDev = 64;
   static int sms_cache[kMaxDev] = {0};
@@ -441,7 +466,7 @@ static int launch_block_t(const void* K16, int ld16, float expo,
     int rows = (int)((budget - Sh::bytes(0)) / (Sh::RB + 8));
     while (rows > 0 && Sh::bytes(rows) > budget) --rows;
     if (rows < 2) return -1;
-    cudaFuncSetAttribute(solve_block_kernel<NQ, kBW, kCPS, RLX>,
+    cudaFuncSetAttribute(solve_block_kernel<NQ, kBW, kCPS, RLX, GRP>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Sh::bytes(rows));
     int sms = 0;
@@ -450,14 +475,50 @@ static int launch_block_t(const void* K16, int ld16, float expo,
     rows_cache[dev] = rows;
   }
   const int rows = rows_cache[dev];
+  const int64_t items = GRP ? t.N * (int64_t)nsrc : t.N;
   int64_t grid = (int64_t)sms_cache[dev] * kCPS;
-  if (grid > t.N) grid = t.N;
+  if (grid > items) grid = items;
   if (grid < 1) grid = 1;
-  solve_block_kernel<NQ, kBW, kCPS, RLX><<<(unsigned)grid, kBW * 32, Sh::bytes(rows), st>>>(
-      static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr,
-      t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows, ctl.omega,
-      ctl.vstate, ctl.mrow, out);
+  solve_block_kernel<NQ, kBW, kCPS, RLX, GRP>
+      <<<(unsigned)grid, kBW * 32, Sh::bytes(rows), st>>>(
+          static_cast<const uint2*>(K16), ld16 / 4, expo, s.vr, s.rinv, t.col_ptr,
+          t.ent, t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, u0, ldu, rows,
+          ctl.omega, ctl.vstate, ctl.mrow, out, grp, nsrc);
   return 1;
+}
+
+// Stacked batch group on the BF16 panels (all of panel width ld16): one
+// persistent launch over every (source, document) pair, in the launch shape
+// `shape` (0: 4 warps x 4 CTAs/SM, 1: 8 x 2, 2: 16 x 1).
+template <int NQ>
+static int launch_block_group_nq(const GroupSrc* grp, int nsrc, int ld16, float expo,
+                                 const Targets& t, const SolveCtl& ctl, int shape,
+                                 cudaStream_t st) {
+  SourceSel none;
+  const bool r = ctl.omega != 1.f;
+  switch (shape) {
+    case 1:
+      return r ? launch_block_t<NQ, 8, 2, true, true>(nullptr, ld16, expo, none, t, ctl, nullptr, 0, nullptr, st, grp, nsrc)
+               : launch_block_t<NQ, 8, 2, false, true>(nullptr, ld16, expo, none, t, ctl, nullptr, 0, nullptr, st, grp, nsrc);
+    case 2:
+      return r ? launch_block_t<NQ, 16, 1, true, true>(nullptr, ld16, expo, none, t, ctl, nullptr, 0, nullptr, st, grp, nsrc)
+               : launch_block_t<NQ, 16, 1, false, true>(nullptr, ld16, expo, none, t, ctl, nullptr, 0, nullptr, st, grp, nsrc);
+    default:
+      return r ? launch_block_t<NQ, 4, 4, true, true>(nullptr, ld16, expo, none, t, ctl, nullptr, 0, nullptr, st, grp, nsrc)
+               : launch_block_t<NQ, 4, 4, false, true>(nullptr, ld16, expo, none, t, ctl, nullptr, 0, nullptr, st, grp, nsrc);
+  }
+}
+
+int launch_block_group(const GroupSrc* grp, int nsrc, int ld16, float expo,
+                       const Targets& t, const SolveCtl& ctl, int shape, cudaStream_t st) {
+  if (t.N <= 0 || nsrc <= 0) return 0;
+  switch (ld16 / 128) {
+    case 1: return launch_block_group_nq<1>(grp, nsrc, ld16, expo, t, ctl, shape, st);
+    case 2: return launch_block_group_nq<2>(grp, nsrc, ld16, expo, t, ctl, shape, st);
+    case 3: return launch_block_group_nq<3>(grp, nsrc, ld16, expo, t, ctl, shape, st);
+    case 4: return launch_block_group_nq<4>(grp, nsrc, ld16, expo, t, ctl, shape, st);
+  }
+  return -1;
 }
 
 // Over-relaxed solves (omega != 1) run the instantiation that keeps each

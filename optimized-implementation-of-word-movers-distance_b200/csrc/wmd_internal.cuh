@@ -158,6 +158,15 @@ int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
 // Returns launches, or -1 if unsupported (tensor maps or shared-memory
 // budget).
 enum TcForm { TC_FP16 = 0, TC_BF16 = 1, TC_TF32X3 = 2 };
+struct GroupSrc;
+// A stacked batch group's cost panel (batch.cu): N-tile y of the launch is
+// tiles[y] = {source, first stacked source row, first panel column, 0}, the
+// sources' panels in src[] (device arrays), nt source rows per tile.
+struct StackedPanels {
+  const int4* tiles = nullptr;
+  const GroupSrc* src = nullptr;
+  int ntiles = 0, nt = 0;
+};
 int tc_padded_width(uint64_t d);
 int tc_tile_n(uint32_t cap, uint64_t d);
 int tc_tile_n_x3(uint32_t cap, uint64_t d);  // 0 = form unsupported
@@ -167,7 +176,8 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
                     const float* E32, const float* nE, uint64_t V, uint64_t d,
                     const SourceSel& s, float expo, float* K, float* KM, int ld,
                     const NearList& near, unsigned* err, int num_sms,
-                    cudaStream_t st, float* mrow = nullptr);
+                    cudaStream_t st, float* mrow = nullptr,
+                    const StackedPanels* grp = nullptr);
 
 // Exact FP32 recompute of the listed near pairs (after either cost panel);
 // pairs beyond the list capacity are recomputed by a full-panel scan.
@@ -300,12 +310,53 @@ struct RelaxGuard {
   }
 };
 
+// One source of a stacked batch group (batch.cu): its panels, weights and
+// outputs, and its place in the stacked source rows.
+struct GroupSrc {
+  float* K = nullptr;          // FP32 panel [V][ld]
+  void* K16 = nullptr;         // BF16 panel [V][ld16] (block solve) or null
+  float* mrow = nullptr;       // row minima (row-scaled panel) or null
+  const float* rinv = nullptr; // [vr] 1 / r_i
+  const uint32_t* vr_dev = nullptr;  // [1] v_r on the device
+  double* out = nullptr;       // [N] scores
+  int* iters = nullptr;        // [N] update counts or null
+  float* vstate = nullptr;     // [nnz] previous v (over-relaxed) or null
+  int vr = 0, ld = 0, row0 = 0, pad = 0;
+};
+
+// Stacked batch group: one persistent warp-solve launch over all (source,
+// document) pairs of nsrc sources with v_r <= vr_max (grp: device array).
+int launch_solve_group(uint32_t vr_max, const GroupSrc* grp, int nsrc, float expo,
+                       const Targets& t, const SolveCtl& ctl, cudaStream_t st);
+
+// Stacked batch groups (batch.cu): stacked source rows (rowword: embedding
+// row per stacked row, -1 = zeros), near-pair fix-up with pairs {word,
+// stacked row} (rowsrc: source of each stacked row), FP32 -> BF16 panels.
+int launch_group_gather(const int32_t* rowword, int rows, const float* E32,
+                        const float* nE, uint64_t d, float* S, float* nS,
+                        const void* E16, void* S16, int dp, int num_sms, cudaStream_t st);
+int launch_near_fixup_group(const NearList& near, float expo, const int32_t* rowsrc,
+                            const GroupSrc* grp, int nsrc, uint64_t V, const float* nE,
+                            const float* nS, int num_sms, cudaStream_t st);
+int launch_panel_to_bf16_group(const GroupSrc* grp, int nsrc, uint64_t V, int ld16,
+                               int num_sms, cudaStream_t st);
+
+// Stacked batch group on BF16 panels of width ld16 (64 < v_r <= 512): one
+// persistent CTA-per-document launch over all (source, document) pairs.
+// shape: 0 = 4 warps x 4 CTAs/SM, 1 = 8 x 2, 2 = 16 x 1.
+int launch_block_group(const GroupSrc* grp, int nsrc, int ld16, float expo,
+                       const Targets& t, const SolveCtl& ctl, int shape, cudaStream_t st);
+
 // Fused Sinkhorn iterations + final half-step + FP64 reduction, one warp per
 // target document.  Returns launches issued (-1 on unsupported vr_cap).
 // KM may be null unless expo == 0.
+// shape: an autotuner candidate of the plain warp solve (0 .. 2, see
+// solve_shape_name) or -1 for the build-time default.
 int launch_solve(const float* K, const float* KM, int ld, float expo,
                  uint32_t vr_cap, const SourceSel& s, const Targets& t,
-                 const SolveCtl& ctl, double* out, cudaStream_t st);
+                 const SolveCtl& ctl, double* out, cudaStream_t st, int shape = -1);
+int solve_shape_count();
+const char* solve_shape_name(int shape);
 
 // Word-major solve (solve_word.cu): the reference's traversal order, each K
 // row read once per pass, u gathered and x scattered (atomics) per entry.

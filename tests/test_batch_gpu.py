@@ -56,3 +56,48 @@ def test_batch_sparse_input_and_validation(wmd, problem):
         eng.query_batch([bad], 10.0, 15)
     assert e.value.name == "WMD_ERR_INVALID_INPUT"
     eng.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+@pytest.mark.parametrize("budget_gib", [32.0, 0.0625])
+def test_stacked_groups_match_per_source(wmd, oracle_mod, problem, prec, budget_gib):
+    """Stacked groups (one cost-panel launch and one persistent solve per
+    group of same-width sources) against the source-by-source pipeline: the
+    same kernels' arithmetic, so the warp-solve classes agree bit for bit and
+    the BF16 block classes within the BF16 panel's bar (the two pipelines may
+    pick different launch shapes); the 64 MiB budget (the smallest allowed)
+    takes the same path with small groups."""
+    vecs, cp, ri, vv, rs = problem
+    eng = wmd.Engine()
+    eng.set_cdist_mode("tf32x3")
+    eng.set_solve_precision(prec)
+    eng.set_embeddings(vecs)
+    eng.set_targets(cp, ri, vv)
+    eng.set_batch_mode(False)
+    ref = eng.query_batch(rs, 10.0, 15)
+    assert eng.last_batch_groups == 0
+    eng.set_batch_mode(True, budget_gib)
+    got = eng.query_batch(rs, 10.0, 15)
+    # four width classes here: v_r <= 32, <= 64, and two wider ones
+    assert eng.last_batch_groups >= 4
+    for k, r in enumerate(rs):
+        vr = int(np.count_nonzero(r))
+        if prec == "bf16" and 64 < vr <= 512:
+            assert rel_err(got[k], ref[k]).max() <= 1e-4
+        else:
+            np.testing.assert_array_equal(got[k], ref[k])
+    # converged, over-relaxed: the same stopping rule in the stacked kernels
+    eng.set_tolerance(1e-4)
+    eng.set_relaxation(1.5)
+    eng.set_batch_mode(False)
+    ref2, it2 = eng.query_batch(rs[:-1], 10.0, 3000, want_iters=True)
+    eng.set_batch_mode(True, budget_gib)
+    got2, itg = eng.query_batch(rs[:-1], 10.0, 3000, want_iters=True)
+    eng.close()
+    E = vecs.astype(np.float64)
+    for k, r in enumerate(rs[:-1]):
+        conv = oracle_mod.sinkhorn_converged(r, E, cp, ri, vv, 10.0, tol=1e-9,
+                                             max_iter_cap=50000)[0]
+        done = itg[k] < 3000
+        assert done.mean() > 0.95
+        assert rel_err(got2[k][done], conv[done]).max() <= 2e-4
