@@ -92,10 +92,17 @@ def args_():
                     help="the batched and warm-start workloads at their full "
                          "sizes: 512 sources; 200k training pairs, 256 "
                          "held-out sources at residual 1e-6 (long)")
+    ap.add_argument("--large-vocab-spec", action="store_true",
+                    help="the large-vocabulary section at its full sizes (1e6 "
+                         "documents, 64 sources; long)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched and converged sections")
     ap.add_argument("--large-vocab", action="store_true",
                     help="add the large-vocabulary section (V=2e6, panel "
                          "streamed from HBM) at a reduced document count")
     a = ap.parse_args()
+    if a.large_vocab_spec:
+        a.large_vocab = True
     if a.spec:
         a.batch_sources, a.held_out, a.conv_tol = 512, 256, 1e-6
         a.ws_train_sources, a.ws_train_pairs, a.oracle_sources = 512, 200_000, 8
@@ -425,9 +432,10 @@ def extras(a, wmd, p, dev):
     # 3. batched queries (the 512-source workload: v_r ~ U[4,512], N = 1e5
     #    targets, 15 iterations) and 4. the converged criterion with the
     #    learned warm start (held-out sources, marginal residual tol)
-    out.update(batched_sections(a, wmd, p, dev))
+    if not a.no_batched:
+        out.update(batched_sections(a, wmd, p, dev))
     if a.large_vocab:
-        out["large_vocab"] = large_vocab(wmd, dev)
+        out["large_vocab"] = large_vocab(a, wmd, dev)
     return out
 
 
@@ -578,61 +586,125 @@ def batched_sections(a, wmd, p, dev):
     return out
 
 
-def large_vocab(wmd, dev):
-    """V = 2e6 words (20000 cluster centres), sources v_r ~ U[16,512],
-    targets nnz ~ U[8,512]; the document count is reduced to 1e5 (from 1e6)
-    to bound the synthetic-data generation time on the host.  BF16 K panel
-    (V x ld16 x 2 bytes, up to 2 GB: far beyond L2, streamed from HBM),
-    15 iterations and at the converged criterion, against the plain FP32
-    path on the same sources."""
+def _compact(E, r, cp, ri, va, docs):
+    """The first `docs` documents of a target set on the vocabulary of their
+    words and the source's words only (the scores depend on no other row):
+    (E_sub float64, r_sub, cp_sub, ri_sub, va_sub)."""
+    c = cp[:docs + 1]
+    rows = ri[:c[-1]]
+    words = np.union1d(np.unique(rows), np.nonzero(r)[0])
+    remap = np.full(E.shape[0], -1, np.int64)
+    remap[words] = np.arange(words.size)
+    return (E[words].astype(np.float64), r[words], c, remap[rows], va[:c[-1]])
+
+
+def large_vocab(a, wmd, dev):
+    """Large vocabulary: V = 2e6 words (20000 cluster centres) given in BF16,
+    sources v_r ~ U[16,512], targets nnz ~ U[8,512]; the K panels (up to 2 GB
+    in BF16 per source) are far beyond L2 and stream from HBM.  Default: 1e5
+    of the 1e6 documents and 4 sources; --spec: all 1e6 documents and 64
+    sources.  At the converged criterion (marginal residual <= 1e-4): the
+    plain FP32 path (FP32-accurate cost panel, FP32 panel) on a subset of the
+    sources against the batched BF16 path (BF16 cost panel and panel, both
+    half-steps relaxed) on all of them, cold and with the learned warm start;
+    every form checked against the converged FP64 oracle on a sample."""
+    import torch
+    import oracle
     synth = importlib.import_module(PKG + ".synth")
-    V, d, N, S = 2_000_000, 300, 100_000, 4
+    spec = a.large_vocab_spec
+    V, d = 2_000_000, 300
+    N, S = (1_000_000, 64) if spec else (100_000, 4)
     t0 = time.perf_counter()
-    E = synth.embeddings(V, d, 20000, seed=0)
+    E16 = torch.from_numpy(synth.embeddings(V, d, 20000, seed=0)).to(torch.bfloat16)
+    Ev = E16.to(torch.float32).numpy()  # the BF16 values
+    cp, ri, va = synth.targets_parallel(V, N, 8, 512, seed=2)
+    rng = np.random.default_rng(9)
     cdf = synth.zipf_cdf(V)
-    cp, ri, va = synth.targets(V, N, 8, 512, seed=2, cdf=cdf)
-    rs, vrs = synth.batched_sources(V, S, 16, 512, seed=9, cdf=cdf)
+    vrs = rng.integers(16, 513, S)
+    rs = [synth.source_doc(V, int(v), seed=9000 + q, cdf=cdf) for q, v in enumerate(vrs)]
     gen = time.perf_counter() - t0
     eng = wmd.Engine(dev.index)
-    eng.set_cdist_mode("tf32x3")  # FP32-accurate cost panel for both arms
-    eng.set_embeddings(E)
+    eng.set_embeddings_bf16(E16)
     eng.set_targets(cp, ri, va)
     res = {"V": V, "docs": N, "nnz": int(cp[-1]), "sources": S, "sum_vr": int(sum(vrs)),
-           "generation_seconds": gen, "cost_panel": "tf32x3 (FP32-accurate, tensor cores)"}
-    for name, prec in (("plain_fp32", "fp32"), ("bf16_panel", "bf16")):
+           "embeddings": "BF16", "generation_seconds": gen,
+           "timing": "device (CUDA events around the batch's kernels)"}
+    tol = 1e-4
+    eng.set_tolerance(tol)
+    # the converged FP64 oracle on a sample (2 sources x 50 documents, on the
+    # vocabulary of their words)
+    ns, nd = 2, 50
+    conv = []
+    for r in rs[:ns]:
+        Es, rsub, c, rr, vv = _compact(Ev, r, cp, ri, va, nd)
+        conv.append(oracle.sinkhorn_converged(rsub, Es, c, rr, vv, 10.0, tol=1e-9,
+                                              max_iter_cap=100000)[0])
+    conv = np.array(conv)
+    P = min(S, 8 if spec else S)  # sources of the plain FP32 path
+
+    def form(name, srcs, mode, prec, omega, params):
+        eng.set_cdist_mode(mode)
         eng.set_solve_precision(prec)
-        eng.set_timing(True)
-        eng.query_batch(_one_per_width(rs), 10.0, 15)
-        t0 = time.perf_counter()
-        out = eng.query_batch(rs, 10.0, 15)
-        dt = time.perf_counter() - t0
-        res[name] = {"pairs_per_s": S * N / dt, "seconds": dt}
-        if prec == "fp32":
-            ref = out
-    res["bf16_panel"]["max_rel_diff_vs_fp32_panel"] = float(np.nanmax(_rel(out, ref)))
-    res["bf16_panel"]["autotuned_shapes"] = {
-        f"ld16={k[0]}{' beyond 64MiB' if k[1] else ''}": v
-        for k, v in eng.autotune_choices().items()}
-    # panel staging bytes the BF16 solve must move at least once per source
+        eng.set_relaxation(omega)
+        eng.set_warm_start(params)
+        (out, its), dt = _device_batch(eng, srcs, 10.0, 20000, want_iters=True)
+        e = _rel(out[:ns, :nd], conv)
+        res[name] = {"sources": len(srcs), "pairs_per_s": len(srcs) * N / dt,
+                     "seconds": dt, "iters_mean": float(its.mean()),
+                     "iters_max": int(its.max()), "groups": eng.last_batch_groups,
+                     "rel_err_vs_converged_fp64": {"max": float(np.nanmax(e)),
+                                                   "median": float(np.nanmedian(e))},
+                     "meets_1e-4": bool(np.nanmax(e) <= 1e-4)}
+        eng.set_relaxation(1.0)
+        eng.set_warm_start(None)
+        return dt
+
+    form("plain_fp32", rs[:P], "tf32x3", "fp32", 1.0, None)
+    dt = form("bf16_batched_omega=1.7", rs, "bf16", "bf16", 1.7, None)
+    res["bf16_batched_omega=1.7"]["speedup_vs_plain_fp32"] = (
+        res["bf16_batched_omega=1.7"]["pairs_per_s"] / res["plain_fp32"]["pairs_per_s"])
+    # HBM roofline of the BF16 solve: every document row of each source's BF16
+    # panel is read at least once (nnz * ld16 * 2 bytes per source)
     nnz = int(cp[-1])
-    bytes_once = sum(nnz * (128 * ((v + 127) // 128)) * 2 for v in vrs)
+    bytes_once = sum(nnz * (128 * ((int(v) + 127) // 128)) * 2 for v in vrs)
     peak, src = measured_peaks()
-    gbs = bytes_once / res["bf16_panel"]["seconds"] / 1e9
-    res["bf16_panel"]["hbm_roofline"] = {
-        "bytes": bytes_once, "bytes_model": "every document row of the BF16 "
-        "panel read once per source (nnz * ld16 * 2), the minimum the solve "
-        "must stream from HBM", "achieved_gbs": gbs, "peak_gbs": peak,
+    gbs = bytes_once / dt / 1e9
+    res["bf16_batched_omega=1.7"]["hbm_roofline"] = {
+        "bytes": bytes_once, "bytes_model": "every document row of each source's "
+        "BF16 panel read once (nnz * ld16 * 2 per source); the rows are re-used "
+        "on chip for all the passes", "achieved_gbs": gbs, "peak_gbs": peak,
         "frac": gbs / peak, "peak_source": src}
-    # the panel beyond L2: the reference's word-major order (each K row
-    # streamed once per pass, u / x through HBM) against the document-major
-    # FP32 solve, one source each, device time
+    if not a.no_warm_start:
+        # the learned warm start, trained on this target set's documents
+        T = 32 if spec else 16
+        train = [synth.source_doc(V, int(v), seed=20000 + q, cdf=cdf)
+                 for q, v in enumerate(rng.integers(16, 513, T))]
+        eng.set_cdist_mode("bf16")
+        t0 = time.perf_counter()
+        info = eng.ws_build_training_set(train, 10.0, docs_per_source=200,
+                                         words_per_doc=16, label_tol=1e-7,
+                                         label_max_iter=3000, seed=3)
+        params, loss = eng.ws_train(wmd.ws_init_params(d, 0), epochs=a.ws_epochs,
+                                    batch_groups=256, lr=3e-3)
+        t_tr = time.perf_counter() - t0
+        form("bf16_warm_omega=1.7", rs, "bf16", "bf16", 1.7, params)
+        res["bf16_warm_omega=1.7"]["speedup_vs_plain_fp32"] = (
+            res["bf16_warm_omega=1.7"]["pairs_per_s"] / res["plain_fp32"]["pairs_per_s"])
+        res["bf16_warm_omega=1.7"]["training"] = {
+            "pairs": info["groups"], "rows": info["rows"], "seconds": t_tr,
+            "loss_last": float(loss[-1])}
+    # the panel beyond L2: the reference's word-major order against the
+    # document-major FP32 solve, one source, 15 iterations
+    eng.set_tolerance(0.0)
+    eng.set_cdist_mode("tf32x3")
     eng.set_solve_precision("fp32")
     wm = {}
     for order in ("document", "word"):
         eng.set_solve_order(order)
         eng.set_timing(True)
         o1 = eng.query(rs[0], 10.0, 15)
-        sel, cd, sv = eng.stage_times()
+        _, _, sv = eng.stage_times()
+        eng.set_timing(False)
         wm[order] = {"solve_ms": sv, "pairs_per_s_solve": N / (sv * 1e-3)}
         if order == "document":
             o_doc = o1
@@ -640,27 +712,6 @@ def large_vocab(wmd, dev):
     wm["word"]["max_rel_diff_vs_document"] = float(np.nanmax(_rel(o1, o_doc)))
     wm["v_r"] = int(vrs[0])
     res["solve_order_one_source"] = wm
-    # at the converged criterion (marginal residual <= 1e-4, WMD within
-    # ~6e-5 of the converged FP64 value): the plain FP32 path against the
-    # BF16 panel with both half-steps over-relaxed
-    eng.set_tolerance(1e-4)
-    conv = {"tol_marginal_residual": 1e-4}
-    for name, prec, om in (("plain_fp32", "fp32", 1.0), ("bf16_panel_omega=1.7", "bf16", 1.7)):
-        eng.set_solve_precision(prec)
-        eng.set_relaxation(om)
-        t0 = time.perf_counter()
-        out, its = eng.query_batch(rs, 10.0, 5000, want_iters=True)
-        dt = time.perf_counter() - t0
-        conv[name] = {"pairs_per_s": S * N / dt, "seconds": dt,
-                      "iters_mean": float(its.mean()), "iters_max": int(its.max())}
-        if prec == "fp32":
-            ref = out
-        else:
-            conv[name]["max_rel_diff_vs_plain_fp32"] = float(np.nanmax(_rel(out, ref)))
-            conv[name]["speedup_vs_plain_fp32"] = conv["plain_fp32"]["seconds"] / dt
-    eng.set_relaxation(1.0)
-    eng.set_tolerance(0.0)
-    res["converged"] = conv
     eng.close()
     return res
 

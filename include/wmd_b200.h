@@ -154,6 +154,14 @@ wmd_status wmd_set_embeddings_f64(wmd_handle* h, const double* vecs, uint64_t V,
 wmd_status wmd_set_embeddings_f32(wmd_handle* h, const float* vecs, uint64_t V,
                                   uint64_t d, int where);
 
+/* Embeddings given in BF16 ([V][d] raw BF16 bit patterns, host (where = 0)
+ * or device (where = 1) memory), no reference counterpart (the reference's
+ * vecs are FP64).  The engine keeps the BF16 rows as the tensor-core copy the
+ * BF16 cost panel reads (wmd_set_cdist_mode(h, WMD_CDIST_BF16)) and their
+ * exact FP32 values for the near-pair recompute and the other forms. */
+wmd_status wmd_set_embeddings_bf16(wmd_handle* h, const uint16_t* vecs, uint64_t V,
+                                   uint64_t d, int where);
+
 /* Target documents (host memory).  Validated on the GPU. */
 wmd_status wmd_set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c);
 wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* c);

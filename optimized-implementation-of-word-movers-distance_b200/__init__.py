@@ -246,6 +246,22 @@ class Engine:
             V, d = a.shape
         self.V, self.d = int(V), int(d)
 
+    def set_embeddings_bf16(self, vecs):
+        """vecs: BF16 embeddings, a torch bfloat16 tensor (CPU or this
+        handle's device) or a numpy uint16 array of raw BF16 bit patterns."""
+        if hasattr(vecs, "data_ptr"):
+            t = vecs.contiguous()
+            V, d = t.shape
+            where = 1 if getattr(t, "is_cuda", False) else 0
+            check(lib().wmd_set_embeddings_bf16(self._h, ctypes.c_void_p(t.data_ptr()),
+                                                V, d, where))
+        else:
+            a = np.ascontiguousarray(vecs, np.uint16)
+            V, d = a.shape
+            check(lib().wmd_set_embeddings_bf16(self._h, a.ctypes.data_as(ctypes.c_void_p),
+                                                V, d, 0))
+        self.V, self.d = int(V), int(d)
+
     def set_targets(self, col_ptr, row_inds, vals, V=None):
         col_ptr, row_inds, vals = _u64(col_ptr), _u64(row_inds), _f64(vals)
         V = self.V if V is None else int(V)

@@ -65,6 +65,8 @@ _SIGS = [
      [ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, ctypes.c_int]),
     ("wmd_set_embeddings_f32", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, ctypes.c_int]),
+    ("wmd_set_embeddings_bf16", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, c_u64, c_u64, ctypes.c_int]),
     ("wmd_set_targets_csc", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSC)]),
     ("wmd_set_targets_csr", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CSR)]),
     ("wmd_set_cdist_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

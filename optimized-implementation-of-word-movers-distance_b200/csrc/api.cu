@@ -1692,6 +1692,44 @@ wmd_status wmd_set_embeddings_f32(wmd_handle* h, const float* vecs, uint64_t V,
   return set_embeddings(h, vecs, V, d, where, false);
 }
 
+wmd_status wmd_set_embeddings_bf16(wmd_handle* h, const uint16_t* vecs, uint64_t V,
+                                   uint64_t d, int where) {
+  if (!h || !vecs || V == 0 || d == 0 || (where != 0 && where != 1))
+    return fail(WMD_ERR_INVALID_ARG, "set_embeddings_bf16: bad argument");
+  if (V > 0xFFFFFFFFull)
+    return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^32 words");
+  if (d > 65536) return fail(WMD_ERR_UNSUPPORTED, "embedding width above 65536");
+  wmd_status s = bind(h);
+  if (s) return s;
+  const size_t n = (size_t)V * d;
+  const int dp = tc_padded_width(d);
+  CK(h->E32.ensure(n * sizeof(float)));
+  CK(h->nE.ensure((size_t)V * sizeof(float)));
+  CK(h->E16.ensure((size_t)V * dp * 2));
+  const void* src = vecs;
+  if (where == 0) {  // host BF16: staged through the FP64 staging buffer
+    CK(h->E64_stage.ensure(n * 2));
+    CK(cudaMemcpyAsync(h->E64_stage.p, vecs, n * 2, cudaMemcpyHostToDevice, h->stream));
+    src = h->E64_stage.p;
+  }
+  int launches = launch_embed_from_bf16(src, V, d, dp, h->E32.as<float>(), h->E16.p,
+                                        h->stream);
+  launches += launch_embed_norms(h->E32.as<float>(), V, d, h->nE.as<float>(), h->stream);
+  s = update_emax(h, V);
+  if (s) return s;
+  CK(cudaGetLastError());
+  h->V = V;
+  h->d = d;
+  h->have_E = true;
+  h->e16_fmt = 1;  // E16 holds the BF16 embeddings themselves
+  h->ws_docs_ready = false;
+  for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
+  h->graph_epoch++;
+  h->last_launches = launches + 1;
+  return WMD_OK;
+}
+
 wmd_status wmd_set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
   return set_targets_csc(h, c);
 }

@@ -57,6 +57,32 @@ int launch_embed_convert_f64(const double* src, uint64_t V, uint64_t d,
   return 1;
 }
 
+// BF16 embeddings [V][d] -> the exact FP32 working copy E32 [V][d] and the
+// tensor-core copy E16 [V][dp] (the same BF16 values, zero-padded to dp).
+__global__ void embed_from_bf16_kernel(const uint16_t* __restrict__ src, uint64_t V,
+                                       int d, int dp, float* __restrict__ E32,
+                                       uint16_t* __restrict__ E16) {
+  const uint64_t total = V * (uint64_t)dp;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t w = i / dp;
+    const int k = (int)(i - w * dp);
+    const uint16_t b = k < d ? src[w * d + k] : (uint16_t)0;
+    E16[i] = b;
+    if (k < d) E32[w * d + k] = __uint_as_float((unsigned)b << 16);
+  }
+}
+
+int launch_embed_from_bf16(const void* src, uint64_t V, uint64_t d, int dp, float* E32,
+                           void* E16, cudaStream_t st) {
+  const uint64_t total = V * (uint64_t)dp;
+  uint64_t blocks = (total + 255) / 256;
+  if (blocks > 65535ull * 16) blocks = 65535ull * 16;
+  embed_from_bf16_kernel<<<(unsigned)blocks, 256, 0, st>>>(
+      static_cast<const uint16_t*>(src), V, (int)d, dp, E32, static_cast<uint16_t*>(E16));
+  return 1;
+}
+
 int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
                        cudaStream_t st) {
   const int threads = 256;

@@ -104,6 +104,9 @@ int launch_embed_convert_f64(const double* src, uint64_t V, uint64_t d,
                              float* E32, float* nE, cudaStream_t st);
 int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
                        cudaStream_t st);
+// BF16 embeddings [V][d] (raw bit patterns) -> E32 (exact) and E16 [V][dp].
+int launch_embed_from_bf16(const void* src, uint64_t V, uint64_t d, int dp, float* E32,
+                           void* E16, cudaStream_t st);
 // Rows of the words a query can touch (target words in `ent`, source words
 // r_dev != 0) read from device-mapped host memory and converted; all other
 // rows zeroed.  `need` is V bytes of scratch; *nrows receives the number of

@@ -157,3 +157,45 @@ def test_end_to_end_gain(wmd, synth, oracle_mod):
     assert it_warm.mean() < it_cold.mean()
     assert it_rx.mean() < it_warm.mean()
     eng.close()
+
+
+def test_gain_on_sources_seen_in_training(wmd, synth, oracle_mod):
+    """What a trained network gains when its predictions are good: trained on
+    the sources it is then asked about (each source's own converged scalings
+    on a sample of the documents), the warm start must cut the updates to a
+    marginal residual of 1e-5 by at least 25 % over the cold start, and the
+    whole query (inference included) must take less device time; the scores
+    stay within 1e-4 of the converged FP64 oracle.  On sources it has not
+    seen (test_end_to_end_gain, the bench's held-out protocol) the same
+    network gains little: its errors lie along the iteration's slow modes."""
+    p = synth.case(4000, 300, 1500, 24, 8, 96, 40, 33)
+    cdf = synth.zipf_cdf(p.V)
+    srcs = [synth.source_doc(p.V, v, seed=700 + v, cdf=cdf) for v in (40, 90, 150)]
+    eng = wmd.Engine()
+    eng.set_embeddings(p.vecs)
+    eng.set_targets(p.col_ptr, p.row_inds, p.vals)
+    eng.ws_build_training_set(srcs, p.lam, docs_per_source=1500, words_per_doc=40,
+                              label_tol=1e-7, label_max_iter=20000, seed=4)
+    params, loss = eng.ws_train(wmd.ws_init_params(300, 3), epochs=60, batch_groups=64,
+                                lr=2e-3)
+    eng.set_tolerance(1e-5)
+    eng.set_batch_mode(False)
+    eng.set_timing(True)
+    cold, it_cold = eng.query_batch(srcs, p.lam, 5000, want_iters=True)
+    t_cold = sum(eng.stage_times())
+    eng.set_warm_start(params)
+    warm, it_warm = eng.query_batch(srcs, p.lam, 5000, want_iters=True)
+    t_warm = sum(eng.stage_times())
+    eng.close()
+    for q, r in enumerate(srcs):
+        conv = oracle_mod.sinkhorn_converged(r, p.vecs.astype(np.float64), p.col_ptr,
+                                             p.row_inds, p.vals, p.lam, tol=1e-9,
+                                             max_iter_cap=50000)[0]
+        done = (it_warm[q] < 5000) & (it_cold[q] < 5000)
+        assert done.mean() > 0.95
+        assert rel_err(warm[q][done], conv[done]).max() <= 1e-4
+    gain = 1.0 - it_warm.mean() / it_cold.mean()
+    print(f"seen sources: updates cold {it_cold.mean():.1f} warm {it_warm.mean():.1f} "
+          f"({100 * gain:.0f} % fewer); device ms cold {t_cold:.2f} warm {t_warm:.2f}")
+    assert gain >= 0.25
+    assert t_warm < t_cold
