@@ -341,12 +341,17 @@ def _rel(a, b):
 
 
 def _one_per_width(rs):
-    """One source of each BF16 panel width class (v_r rounded up to 128), so
-    that a warm-up call leaves the one-time launch-shape tuning of every class
-    out of the timed call."""
+    """One source of each width class (BF16 panel width: v_r rounded up to
+    128; warp-solve lane layout: v_r rounded up to 32 * 2^k), so that a
+    warm-up call leaves the one-time launch-shape tuning of every class out of
+    the timed call."""
     seen, out = set(), []
     for r in rs:
-        w = (np.count_nonzero(r) + 127) // 128
+        v = int(np.count_nonzero(r))
+        k = 0
+        while k < 5 and (32 << k) < v:
+            k += 1
+        w = ((v + 127) // 128, k)
         if w not in seen:
             seen.add(w)
             out.append(r)

@@ -215,6 +215,14 @@ int wmd_last_batch_groups(wmd_handle* h);
 wmd_status wmd_solve_shape_choices(wmd_handle* h, int* shapes);
 const char* wmd_solve_shape_name(int shape);
 
+/* Launch shapes chosen for the stacked batch solves (each timed on the first
+ * group of its class, 4 updates): shapes[0..3] the stacked block solve per
+ * BF16 panel width 128, 256, 384, 512 (names: wmd_block_shape_name, 0-2),
+ * shapes[4..9] the stacked warp solve per lane layout v_r <= 32 .. 1024
+ * (names: wmd_solve_shape_name); -2 = not tuned yet.  No reference
+ * counterpart. */
+wmd_status wmd_group_shape_choices(wmd_handle* h, int* shapes);
+
 /* Launch-shape autotuner of the BF16 block solve (on by default): the first
  * solve of each panel width (and panel size class: within / beyond 64 MiB)
  * times every candidate shape on the handle's real data and keeps the

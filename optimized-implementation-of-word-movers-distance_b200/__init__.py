@@ -348,6 +348,20 @@ class Engine:
         return {32 << i: lib().wmd_solve_shape_name(v).decode()
                 for i, v in enumerate(a) if v != -2}
 
+    def group_shape_choices(self) -> dict:
+        """Launch shapes of the stacked batch solves: {("block", panel width)
+        or ("warp", largest v_r of the lane layout): shape name}."""
+        a = (ctypes.c_int * 10)()
+        check(lib().wmd_group_shape_choices(self._h, a))
+        out = {}
+        for i in range(4):
+            if a[i] != -2:
+                out[("block", 128 * (i + 1))] = lib().wmd_block_shape_name(a[i]).decode()
+        for i in range(6):
+            if a[4 + i] != -2:
+                out[("warp", 32 << i)] = lib().wmd_solve_shape_name(a[4 + i]).decode()
+        return out
+
     @property
     def last_batch_groups(self) -> int:
         return int(lib().wmd_last_batch_groups(self._h))

@@ -75,6 +75,7 @@ _SIGS = [
     ("wmd_set_batch_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]),
     ("wmd_last_batch_groups", ctypes.c_int, [ctypes.c_void_p]),
     ("wmd_solve_shape_choices", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    ("wmd_group_shape_choices", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("wmd_solve_shape_name", ctypes.c_char_p, [ctypes.c_int]),
     ("wmd_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("wmd_set_relaxation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

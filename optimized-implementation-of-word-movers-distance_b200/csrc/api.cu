@@ -161,6 +161,7 @@ struct wmd_handle {
   uint64_t group_budget = 32ull << 30;
   DevBuf g_pool, g_pool16, g_vst, g_S, g_nS, g_S16, g_rowword, g_rowsrc, g_tiles, g_src;
   int grp_shape[4] = {-2, -2, -2, -2};
+  int wgrp_shape[6] = {-2, -2, -2, -2, -2, -2};  // stacked warp solve, per lane layout
   int last_groups = 0;
   bool wm_ready = false;
   DevBuf wm_rp, wm_ent, wm_u, wm_x;
@@ -922,6 +923,38 @@ wmd_status topk_device(wmd_handle* h, const double* scores_dev, uint64_t n,
   return WMD_OK;
 }
 
+// Launch shape of a stacked solve: each of n candidates is run once (its
+// first use) and then timed twice with CUDA events on the handle's stream;
+// the one with the smallest time is returned (0 when none could be timed).  `launch(shape)` returns
+// < 0 when a shape is unavailable.
+template <class F>
+int tune_group_shape(wmd_handle* h, int n, F&& launch) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    if (a) cudaEventDestroy(a);
+    return 0;
+  }
+  float best = 1e30f;
+  int bi = 0;
+  for (int sh = 0; sh < n; ++sh) {
+    if (launch(sh) < 0) continue;
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaEventRecord(a, h->stream);
+      launch(sh);
+      cudaEventRecord(b, h->stream);
+      float ms = 0.f;
+      if (cudaEventSynchronize(b) == cudaSuccess &&
+          cudaEventElapsedTime(&ms, a, b) == cudaSuccess && ms < best) {
+        best = ms;
+        bi = sh;
+      }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return bi;
+}
+
 // Many sparse source documents against the resident target set.  Source s
 // holds words src_ids[src_ptr[s] .. src_ptr[s+1]) (strictly ascending, < V)
 // with weights src_w (> 0): the reference's select order (fused:45-63)
@@ -1100,30 +1133,27 @@ wmd_status query_batch_stacked(wmd_handle* h, uint64_t S, const uint64_t* src_pt
           c2.max_iter = 4;
           c2.tol = 0.f;
           c2.omega = 1.f;
-          cudaEvent_t a = nullptr, b = nullptr;
-          CK(cudaEventCreate(&a));
-          CK(cudaEventCreate(&b));
-          float best = 1e30f;
-          int bi = 0;
-          for (int sh = 0; sh < 3; ++sh) {
-            if (launch_block_group(sp.src, ng, l16, expo, t, c2, sh, h->stream) < 0) continue;
-            cudaEventRecord(a, h->stream);
-            launch_block_group(sp.src, ng, l16, expo, t, c2, sh, h->stream);
-            cudaEventRecord(b, h->stream);
-            float ms = 0.f;
-            if (cudaEventSynchronize(b) == cudaSuccess &&
-                cudaEventElapsedTime(&ms, a, b) == cudaSuccess && ms < best) {
-              best = ms;
-              bi = sh;
-            }
-          }
-          cudaEventDestroy(a);
-          cudaEventDestroy(b);
-          shp = bi;
+          shp = tune_group_shape(h, 3, [&](int sh) {
+            return launch_block_group(sp.src, ng, l16, expo, t, c2, sh, h->stream);
+          });
         }
         ls = launch_block_group(sp.src, ng, l16, expo, t, ctl, shp, h->stream);
       } else {
-        ls = launch_solve_group(vmax, sp.src, ng, expo, t, ctl, h->stream);
+        int k = 0;
+        while (k < 5 && (32u << k) < vmax) ++k;
+        int& shp = h->wgrp_shape[k];
+        if (shp == -2 && ctl.omega == 1.f) {
+          // the same for the stacked warp solve (unrelaxed; the relaxed
+          // solve keeps the build-time shape)
+          SolveCtl c2 = ctl;
+          c2.max_iter = 4;
+          c2.tol = 0.f;
+          shp = tune_group_shape(h, solve_shape_count(), [&](int sh) {
+            return launch_solve_group(vmax, sp.src, ng, expo, t, c2, h->stream, sh);
+          });
+        }
+        ls = launch_solve_group(vmax, sp.src, ng, expo, t, ctl, h->stream,
+                                ctl.omega == 1.f ? shp : -1);
       }
       if (ls < 0) return fail(WMD_ERR_UNSUPPORTED, "stacked solve unavailable");
       launches += ls;
@@ -1813,6 +1843,13 @@ wmd_status wmd_solve_shape_choices(wmd_handle* h, int* shapes) {
 }
 
 const char* wmd_solve_shape_name(int shape) { return solve_shape_name(shape); }
+
+wmd_status wmd_group_shape_choices(wmd_handle* h, int* shapes) {
+  if (!h || !shapes) return fail(WMD_ERR_INVALID_ARG, "null argument");
+  for (int i = 0; i < 4; ++i) shapes[i] = h->grp_shape[i];
+  for (int i = 0; i < 6; ++i) shapes[4 + i] = h->wgrp_shape[i];
+  return WMD_OK;
+}
 
 wmd_status wmd_set_solve_order(wmd_handle* h, int order) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");

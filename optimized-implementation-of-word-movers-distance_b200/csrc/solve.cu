@@ -156,7 +156,7 @@ struct SolveShape {
 template <int LPW, bool FROM_KM, bool RLX, bool GRP, int kW = SolveCfg<LPW>::kWarps,
           int kC = SolveCfg<LPW>::kCtas>
 __global__ void __launch_bounds__(kW * 32, kC)
-solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
+solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_arg,
              float expo, const uint32_t* __restrict__ vr_dev,
              const float* __restrict__ rinv,
              const int64_t* __restrict__ col_ptr,
@@ -178,8 +178,24 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   float* red = reinterpret_cast<float*>(wbase + Sh::staged_bytes(srounds) +
                                         Sh::entries_bytes(srounds));
   float* ubuf = red + 32 * 32;
-  int vr = GRP ? 0 : (int)*vr_dev;
-  int ldc = ld >> 2;  // float4 chunks per global panel row
+  // GRP: the current source's arguments, one copy per warp in shared
+  // memory, read where they are used instead of being held in registers for
+  // the whole document loop (which spilled the wide instantiations).
+  __shared__ __align__(16) unsigned char gs_raw[GRP ? kW * sizeof(GroupSrc) : 16];
+  GroupSrc& gs = reinterpret_cast<GroupSrc*>(gs_raw)[GRP ? warp : 0];
+  const int vr_arg = GRP ? 0 : (int)*vr_dev;
+  auto KP = [&]() -> const float* {
+    if constexpr (GRP) return gs.K;
+    else return K;
+  };
+  auto VSTATE = [&]() -> float* {
+    if constexpr (GRP) return gs.vstate;
+    else return vstate;
+  };
+  auto MROW = [&]() -> const float* {
+    if constexpr (GRP) return gs.mrow;
+    else return mrow;
+  };
   // Staged row s holds logical chunk 8q'+t at 8q' + (t ^ ((s*LPW + q') & 7)).
   // For the lane that reads it s*LPW + q = 32*round + lane, so the key is
   // lane & 7: constant per lane, and the 8 lanes of a shared-memory phase hit
@@ -194,12 +210,14 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
   float rv[LPW], rw[LPW];  // 1/r_i and r_i
   unsigned dmask = 0;
   auto set_dims = [&]() {
+    const int vr = GRP ? gs.vr : vr_arg;
+    const float* ri = GRP ? gs.rinv : rinv;
     dmask = 0;
 #pragma unroll
     for (int qq = 0; qq < LPW; ++qq) {
       const int D = 32 * qq + own;
       const bool ok = D < vr;
-      rv[qq] = ok ? rinv[D] : 0.f;
+      rv[qq] = ok ? ri[D] : 0.f;
       rw[qq] = ok ? __frcp_rn(rv[qq]) : 0.f;
       dmask |= ok ? (1u << qq) : 0u;
     }
@@ -241,20 +259,17 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     if constexpr (GRP) {
       const int src = (int)(idx / N);
       if (src != cur_src) {  // this source's panel, weights and outputs
-        const GroupSrc& gs = grp[src];
-        K = gs.K;
-        ld = gs.ld;
-        ldc = ld >> 2;
-        vr = gs.vr;
-        rinv = gs.rinv;
-        iters_out = gs.iters;
-        vstate = gs.vstate;
-        mrow = gs.mrow;
-        out = gs.out;
+        __syncwarp();
+        if (lane == 0) gs = grp[src];
+        __syncwarp();
         set_dims();
         cur_src = src;
       }
     }
+    const int vr = GRP ? gs.vr : vr_arg;
+    const int ld = GRP ? gs.ld : ld_arg;
+    const int ldc = ld >> 2;  // float4 chunks per global panel row
+    const float* const Kd = KP();  // this source's panel
     RelaxGuard rg;  // over-relaxation of this document (RLX instantiations)
     rg.init(omega);
     float resv = 0.f;  // this lane's c-side residual of the current pass
@@ -286,7 +301,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
         zero_row(reg[t]);
         const uint2 en = sE[k];
         creg[t] = __uint_as_float(en.y);
-        const float4* rp = reinterpret_cast<const float4*>(K + (size_t)en.x * ld);
+        const float4* rp = reinterpret_cast<const float4*>(Kd + (size_t)en.x * ld);
 #pragma unroll
         for (int c = 0; c < 8; ++c)
           if (8 * q + c < ldc) reg[t].c[c] = __ldg(rp + 8 * q + c);
@@ -303,7 +318,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
                         : sK + (size_t)s * Sh::NCH + 8 * (lc >> 3) +
                               ((lc & 7) ^ ((s * LPW + (lc >> 3)) & 7));
       if (k < n && lc < ldc)
-        cp_async16(dst, K + (size_t)sE[k].x * ld + 4 * lc);
+        cp_async16(dst, Kd + (size_t)sE[k].x * ld + 4 * lc);
       else
         *dst = k < n ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(1.f, 1.f, 1.f, 1.f);
     }
@@ -392,7 +407,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
     // (vold, prefetched by vold_at with the word's row), which lane q = 0 of
     // the word's group keeps in vstate and broadcasts.
     auto vold_at = [&](int k) -> float {
-      if constexpr (RLX) return (q == 0 && k < n && !rg.vfirst) ? vstate[b + k] : 0.f;
+      if constexpr (RLX) return (q == 0 && k < n && !rg.vfirst) ? VSTATE()[b + k] : 0.f;
       else return 0.f;
     };
     auto vweight = [&](float c, float s, int k, float vold) -> float {
@@ -401,7 +416,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       } else {
         float v = 0.f;
         if (q == 0 && k < n)
-          v = relaxed_v_pre(c, s, vold, vstate + b + k, rg.vfirst, rg.omega, resv);
+          v = relaxed_v_pre(c, s, vold, VSTATE() + b + k, rg.vfirst, rg.omega, resv);
         if constexpr (LPW > 1) v = __shfl_sync(0xffffffffu, v, lane & ~(LPW - 1));
         return v;
       }
@@ -512,7 +527,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       for (int l = 0; l < lr; ++l) {
         Row ra;
         float ca;
-        load_global(K, (rr + sr + l) * WPS + g, ra, ca, true);
+        load_global(Kd, (rr + sr + l) * WPS + g, ra, ca, true);
         const float oa = vold_at((rr + sr + l) * WPS + g);
         axpy(ra, vweight(ca, dot(ra, u2), (rr + sr + l) * WPS + g, oa), x2);
       }
@@ -590,7 +605,8 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       }
       broadcast_u(uval, u2);
     }
-    if (iters_out && lane == 0) iters_out[j] = it;
+    int* const iters_p = GRP ? gs.iters : iters_out;
+    if (iters_p && lane == 0) iters_p[j] = it;
 
     // Final half-step (fused:339-393): WMD = sum_k v_k (KM_k . u), FP64 sum.
     const float km_scale = FROM_KM ? 1.f : 0.69314718f / expo;  // ln 2 / expo
@@ -611,7 +627,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       } else if (t < rr + sr) {
         load_staged(t - rr, rk, ck);
       } else {
-        load_global(K, k, rk, ck, true);
+        load_global(Kd, k, rk, ck, true);
       }
       const float v = weight(ck, dot(rk, u2));
       float tk;
@@ -643,9 +659,9 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       }
       if (q == 0 && k < n) {
         acc += (double)v * (double)tk;
-        if (mrow) {  // row-scaled panel: + c_w m_w (panel_rescale.cu)
+        if (MROW()) {  // row-scaled panel: + c_w m_w (panel_rescale.cu)
           const uint32_t id = k < ne ? sE[k].x : __ldg(&ent[b + k]).x;
-          acc += (double)ck * (double)__ldg(&mrow[id]);
+          acc += (double)ck * (double)__ldg(&MROW()[id]);
         }
       }
     }
@@ -662,12 +678,12 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld,
       // Row-scaled panel: a u this large means a source word whose K entries
       // in this document are at the FP32 floor (subnormal, few significant
       // bits): the document goes to the FP64 re-solve (exact_f64.cu).
-      if (mrow)
+      if (MROW())
         bad |= (d0 < vr && u2[t].x > kScaledUMax) || (d0 + 1 < vr && u2[t].y > kScaledUMax);
     }
     if (__any_sync(0xffffffffu, bad)) acc = __longlong_as_double(0x7ff8000000000000ll);
     if (vr == 0) acc = 0.0;  // no source word: an empty sum (fused:387)
-    if (lane == 0) out[j] = acc;
+    if (lane == 0) (GRP ? gs.out : out)[j] = acc;
     j = jn;
     b = bn;
     n = nn;
@@ -723,26 +739,37 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
 // major so that the grid works on one or two sources' panels at a time.
 template <int LPW>
 static int launch_group_t(const GroupSrc* grp, int nsrc, float expo, const Targets& t,
-                          const SolveCtl& ctl, cudaStream_t st) {
+                          const SolveCtl& ctl, cudaStream_t st, int shape) {
   SourceSel none;
   if (ctl.omega != 1.f)
     return launch_solve_t<LPW, false, true, true>(nullptr, nullptr, 4, expo, none, t, ctl,
                                                   nullptr, st, grp, nsrc);
+  switch (shape) {  // the candidates of solve_shape_name()
+    case 0:
+      return launch_solve_t<LPW, false, false, true, 1, 8>(nullptr, nullptr, 4, expo, none, t,
+                                                           ctl, nullptr, st, grp, nsrc);
+    case 1:
+      return launch_solve_t<LPW, false, false, true, 2, 4>(nullptr, nullptr, 4, expo, none, t,
+                                                           ctl, nullptr, st, grp, nsrc);
+    case 2:
+      return launch_solve_t<LPW, false, false, true, 4, 2>(nullptr, nullptr, 4, expo, none, t,
+                                                           ctl, nullptr, st, grp, nsrc);
+  }
   return launch_solve_t<LPW, false, false, true>(nullptr, nullptr, 4, expo, none, t, ctl,
                                                  nullptr, st, grp, nsrc);
 }
 
 int launch_solve_group(uint32_t vr_max, const GroupSrc* grp, int nsrc, float expo,
-                       const Targets& t, const SolveCtl& ctl, cudaStream_t st) {
+                       const Targets& t, const SolveCtl& ctl, cudaStream_t st, int shape) {
   if (t.N <= 0 || nsrc <= 0) return 0;
   SolveCtl c = ctl;
   c.u0 = nullptr;  // cold start only in the stacked form
-  if (vr_max <= 32) return launch_group_t<1>(grp, nsrc, expo, t, c, st);
-  if (vr_max <= 64) return launch_group_t<2>(grp, nsrc, expo, t, c, st);
-  if (vr_max <= 128) return launch_group_t<4>(grp, nsrc, expo, t, c, st);
-  if (vr_max <= 256) return launch_group_t<8>(grp, nsrc, expo, t, c, st);
-  if (vr_max <= 512) return launch_group_t<16>(grp, nsrc, expo, t, c, st);
-  if (vr_max <= 1024) return launch_group_t<32>(grp, nsrc, expo, t, c, st);
+  if (vr_max <= 32) return launch_group_t<1>(grp, nsrc, expo, t, c, st, shape);
+  if (vr_max <= 64) return launch_group_t<2>(grp, nsrc, expo, t, c, st, shape);
+  if (vr_max <= 128) return launch_group_t<4>(grp, nsrc, expo, t, c, st, shape);
+  if (vr_max <= 256) return launch_group_t<8>(grp, nsrc, expo, t, c, st, shape);
+  if (vr_max <= 512) return launch_group_t<16>(grp, nsrc, expo, t, c, st, shape);
+  if (vr_max <= 1024) return launch_group_t<32>(grp, nsrc, expo, t, c, st, shape);
   return -1;
 }
 

@@ -117,14 +117,37 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
   double* red = reinterpret_cast<double*>(ubufB + RL);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool lo = lane < 16;
-  int vr = GRP ? 0 : (int)*vr_dev;
+  // GRP: the current source's arguments, one copy per CTA in shared memory,
+  // read where they are used instead of being held in registers for the
+  // whole document loop (which spilled the widest instantiation).
+  __shared__ __align__(16) unsigned char gs_raw[GRP ? sizeof(GroupSrc) : 16];
+  GroupSrc& gs = *reinterpret_cast<GroupSrc*>(gs_raw);
+  const int vr_arg = GRP ? 0 : (int)*vr_dev;
+  auto VR = [&]() -> int {
+    if constexpr (GRP) return gs.vr;
+    else return vr_arg;
+  };
+  auto KP = [&]() -> const uint2* {
+    if constexpr (GRP) return static_cast<const uint2*>(gs.K16);
+    else return K16;
+  };
+  auto VSTATE = [&]() -> float* {
+    if constexpr (GRP) return gs.vstate;
+    else return vstate;
+  };
+  auto MROW = [&]() -> const float* {
+    if constexpr (GRP) return gs.mrow;
+    else return mrow;
+  };
 
   float rv[DPT], rw[DPT];  // 1/r_i and r_i of this thread's update dimensions
   auto set_dims = [&]() {
+    const int vr = VR();
+    const float* ri = GRP ? gs.rinv : rinv;
 #pragma unroll
     for (int i = 0; i < DPT; ++i) {
       const int D = tid + i * kBT;
-      rv[i] = D < vr ? rinv[D] : 0.f;
+      rv[i] = D < vr ? ri[D] : 0.f;
       rw[i] = D < vr ? __frcp_rn(rv[i]) : 0.f;
     }
   };
@@ -133,21 +156,6 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
   const int64_t NI = GRP ? N * (int64_t)nsrc : N;  // work items
 
   for (int64_t idx = blockIdx.x; idx < NI; idx += gridDim.x) {
-    if constexpr (GRP) {
-      const int src = (int)(idx / N);
-      if (src != cur_src) {  // this source's panel, weights and outputs
-        const GroupSrc& gs = grp[src];
-        K16 = static_cast<const uint2*>(gs.K16);
-        vr = gs.vr;
-        rinv = gs.rinv;
-        iters_out = gs.iters;
-        vstate = gs.vstate;
-        mrow = gs.mrow;
-        out = gs.out;
-        set_dims();
-        cur_src = src;
-      }
-    }
     const int64_t pos = GRP ? idx % N : idx;
     const int64_t j = order ? (int64_t)order[pos] : pos;
     const int64_t b = col_ptr[j];
@@ -162,6 +170,17 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     float resv = 0.f;  // this thread's c-side residual of the current pass
 
     __syncthreads();  // the previous document is done with shared memory
+    if constexpr (GRP) {
+      const int src = (int)(idx / N);
+      if (src != cur_src) {  // this source's panel, weights and outputs
+        if (tid == 0) gs = grp[src];
+        __syncthreads();
+        set_dims();
+        cur_src = src;
+      }
+    }
+    const int vr = VR();
+    const uint2* const Kd = KP();  // this source's panel (rows past the staged ones)
     for (int k = tid; k < ns; k += kBT) sEnt[k] = __ldg(&ent[b + k]);
     for (int D = tid; D < RL; D += kBT) {
       ubufA[D] = D < vr ? (float)vr : 0.f;  // cold start (fused:188-191)
@@ -171,7 +190,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     for (int c = tid; c < ns * (QPR / 2); c += kBT) {
       const int k = c / (QPR / 2), ch = c % (QPR / 2);
       bcp_async16(sRows + (size_t)k * QPR + 2 * ch,
-                  K16 + (size_t)sEnt[k].x * ldq + 2 * ch);
+                  Kd + (size_t)sEnt[k].x * ldq + 2 * ch);
     }
     bcp_async_wait_all();
     __syncthreads();
@@ -192,7 +211,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       } else {
         const uint2 e = __ldg(&ent[b + k]);
         c = __uint_as_float(e.y);
-        const uint2* rp = K16 + (size_t)e.x * ldq;
+        const uint2* rp = Kd + (size_t)e.x * ldq;
 #pragma unroll
         for (int t = 0; t < NQ; ++t) q[t] = __ldg(rp + lane + 32 * t);
       }
@@ -222,7 +241,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     // every lane.  Relaxed: lanes 0 and 16 own the rows' states (vold: the
     // row's previous v, prefetched by vold_of).
     auto vold_of = [&](int kr) -> float {
-      return (relax && !g.vfirst && (lane & 15) == 0 && kr < r1) ? vstate[b + kr] : 0.f;
+      return (relax && !g.vfirst && (lane & 15) == 0 && kr < r1) ? VSTATE()[b + kr] : 0.f;
     };
     auto pair_weights = [&](float s, float ca, float cb, int ka, float vold, float2& va,
                             float2& vb) {
@@ -230,7 +249,7 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       if (relax) {
         float v = 0.f;
         if ((lane & 15) == 0)
-          v = relaxed_v_pre(lo ? ca : cb, s, vold, vstate + b + ka + (lo ? 0 : 1),
+          v = relaxed_v_pre(lo ? ca : cb, s, vold, VSTATE() + b + ka + (lo ? 0 : 1),
                             g.vfirst, g.omega, resv);
         vm = __shfl_sync(0xffffffffu, v, lane & 16);
       } else {
@@ -358,7 +377,8 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
         __syncthreads();
       }
     }
-    if (iters_out && tid == 0) iters_out[j] = it;
+    int* const iters_p = GRP ? gs.iters : iters_out;
+    if (iters_p && tid == 0) iters_p[j] = it;
 
     // Final half-step (fused:339-393): WMD = sum_k v_k (KM_k . u), FP64 sum,
     // KM_k = K_k ln(K_k) / expo from the staged BF16 row.
@@ -391,9 +411,9 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
       const float tk = pair_sum(kmdot(qa), kmdot(qb)) * km_scale;
       if (lane == 0 || (lane == 16 && k + 1 < r1)) {
         acc += (double)v * (double)tk;
-        if (mrow)  // row-scaled panel: + c_w m_w (panel_rescale.cu)
+        if (MROW())  // row-scaled panel: + c_w m_w (panel_rescale.cu)
           acc += (double)(lo ? ca : cb) *
-                 (double)__ldg(&mrow[__ldg(&ent[b + k + (lo ? 0 : 1)]).x]);
+                 (double)__ldg(&MROW()[__ldg(&ent[b + k + (lo ? 0 : 1)]).x]);
       }
     }
 #pragma unroll
@@ -402,14 +422,14 @@ solve_block_kernel(const uint2* __restrict__ K16, int ldq, float expo,
     // sum over dimensions NaN (fused:382-393).
     bool bad = false;
     for (int D = tid; D < vr; D += kBT)
-      bad |= !isfinite(cur[D]) || (mrow && cur[D] > kScaledUMax);  // see solve.cu
+      bad |= !isfinite(cur[D]) || (MROW() && cur[D] > kScaledUMax);  // see solve.cu
     __syncthreads();  // every warp has read the last u before red is reused
     if (lane == 0) red[warp] = acc;
     bad = __syncthreads_or(bad);
     if (tid == 0) {
       double tot = 0.0;
       for (int w = 0; w < kBW; ++w) tot += red[w];
-      out[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : tot;
+      (GRP ? gs.out : out)[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : tot;
     }
   }
 }

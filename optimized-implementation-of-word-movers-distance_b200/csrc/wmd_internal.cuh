@@ -329,8 +329,11 @@ struct GroupSrc {
 
 // Stacked batch group: one persistent warp-solve launch over all (source,
 // document) pairs of nsrc sources with v_r <= vr_max (grp: device array).
+// shape: launch shape of the unrelaxed solve (0 .. solve_shape_count() - 1,
+// as for launch_solve), -1 the build-time default.
 int launch_solve_group(uint32_t vr_max, const GroupSrc* grp, int nsrc, float expo,
-                       const Targets& t, const SolveCtl& ctl, cudaStream_t st);
+                       const Targets& t, const SolveCtl& ctl, cudaStream_t st,
+                       int shape = -1);
 
 // Stacked batch groups (batch.cu): stacked source rows (rowword: embedding
 // row per stacked row, -1 = zeros), near-pair fix-up with pairs {word,
