@@ -1555,6 +1555,13 @@ wmd_status default_handle(wmd_handle** out) {
     // products); widths it cannot tile (d % 4 != 0) take the FP32 CUDA-core
     // panel.  Both hold the plain path's 1e-5 against the reference.
     tl_handle.h->mode = WMD_CDIST_TF32X3;
+    // Every drop-in call brings a new target set and embeddings, so nothing
+    // that pays off over repeated queries is kept: the launch shapes are the
+    // build-time defaults (the autotuner would re-time its candidates on
+    // every call) and the kernels are launched directly (a captured graph
+    // would be re-captured and instantiated on every call).
+    tl_handle.h->autotune = false;
+    tl_handle.h->use_graphs = false;
   }
   *out = tl_handle.h;
   return WMD_OK;
