@@ -12,13 +12,13 @@ collective).
 
 Our arm prints one JSON line: ``value`` is WMD pairs/s with inputs resident in
 HBM (select + cost panel + fused Sinkhorn solve, CUDA events on the library's
-stream, L2 flushed between steps; the cost panel runs on tcgen05 from the FP32
-embeddings split into TF32 high + low parts, FP32-accurate and checked against
-the oracle at 1e-5 before timing; ``--cdist fp32`` times the CUDA-core panel
-instead); ``e2e`` is the same metric through the
-drop-in C ABI call with pinned host buffers (inside every step: H2D of r and
-the CSC matrix, the GPU's reads of the FP64 embedding rows of the words in the
-targets or the source straight from the pinned buffer, D2H of WMD;
+stream, L2 flushed between steps; the cost panel runs on tcgen05 from a
+resident split-FP16 copy of the embeddings, FP32-accurate and checked against
+the oracle at 1e-5 before timing; ``--cdist`` selects the other forms); ``e2e``
+is the same metric through the drop-in C ABI call with pinned host buffers
+(inside every step: H2D of r and the CSC matrix, the embedding rows of the
+words in the targets or the source narrowed FP64 -> FP32 by the host threads
+and copied while the next rows are converted, D2H of WMD;
 ``h2d_bytes_per_step`` counts what crossed the bus); ``roofline`` covers the
 dominant kernel; ``cpu_baseline`` times the reference's own OpenMP solver on
 this host.  ``--impl reference`` times only the reference's CPU solver.
@@ -59,12 +59,15 @@ def args_():
                     help="time budget of the CPU-baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cdist", choices=["tf32x3", "fp32", "fp16", "bf16"],
-                    default="tf32x3",
-                    help="cost-panel form: tf32x3 (plain form, the default: "
-                         "tcgen05 on the FP32 embeddings split into TF32 high "
-                         "+ low parts, FP32-accurate), fp32 (plain form on "
-                         "CUDA cores) or tcgen05 with 16-bit operands")
+    ap.add_argument("--cdist", choices=["f16x3", "tf32x3", "fp32", "fp16", "bf16"],
+                    default="f16x3",
+                    help="cost-panel form: f16x3 (plain form, the default: "
+                         "tcgen05 on a resident split-FP16 copy of the "
+                         "embeddings, FP16 high part + scaled remainder per "
+                         "row, FP32-accurate), tf32x3 (tcgen05 on the FP32 "
+                         "embeddings split into TF32 high + low parts in the "
+                         "kernel, FP32-accurate), fp32 (plain form on CUDA "
+                         "cores) or tcgen05 with 16-bit operands")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the precision-form, converged and batched / "
                          "warm-start sections (single GPU only)")
@@ -387,7 +390,7 @@ def extras(a, wmd, p, dev):
     r_dev = torch.from_numpy(p.r).to(dev)
     o = torch.empty(p.N, dtype=torch.float64, device=dev)
     forms = {}
-    for mode in ("fp32", "tf32x3", "fp16", "bf16"):
+    for mode in ("fp32", "tf32x3", "f16x3", "fp16", "bf16"):
         eng.set_cdist_mode(mode)
         fn = lambda: eng.query_device(r_dev.data_ptr(), W["v_r"], p.lam, p.max_iter,
                                       o.data_ptr())
@@ -775,7 +778,7 @@ def ours(a, rank, world, local):
                           p.max_iter)
     got = out[:sub].cpu().numpy()
     max_rel = float(np.max(np.abs(got - ref) / np.abs(ref)))
-    tol = {"fp32": 1e-5, "tf32x3": 1e-5, "fp16": 1e-4, "bf16": 1e-3}[a.cdist]
+    tol = {"fp32": 1e-5, "tf32x3": 1e-5, "f16x3": 1e-5, "fp16": 1e-4, "bf16": 1e-3}[a.cdist]
     if not max_rel <= tol:
         raise SystemExit(f"bench: result check failed, max rel err {max_rel:.3e}")
 
@@ -849,10 +852,12 @@ def ours(a, rank, world, local):
     peak_hbm, peak_src = measured_peaks()
     sm_mhz = clocks.get("sm_mhz") or 1965.0
     fp32_nominal = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-    cd_name = {"fp32": "cdist_fp32_kernel", "tf32x3": "cdist_tc_kernel_tf32x3"}.get(
-        a.cdist, "cdist_tc_kernel")
+    cd_name = {"fp32": "cdist_fp32_kernel", "tf32x3": "cdist_tc_kernel_tf32x3",
+               "f16x3": "cdist_tc_kernel_f16x3"}.get(a.cdist, "cdist_tc_kernel")
     if a.cdist in ("fp16", "bf16"):
         cdist_bytes = V * ((d + 7) // 8 * 8) * 2 + 2 * vr * V * 4
+    elif a.cdist == "f16x3":  # split rows: 4 * dp + 16 bytes per word
+        cdist_bytes = V * (4 * ((d + 7) // 8 * 8) + 16) + 2 * vr * V * 4
     dominant = "solve_kernel" if sv_ms >= cd_ms else cd_name
     if dominant == "solve_kernel":
         # The solve gathers each document's K rows once from the L2-resident
@@ -945,6 +950,18 @@ def ours(a, rank, world, local):
     if world > 1:
         dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
         dist.all_reduce(res_tot, op=dist.ReduceOp.MAX)
+    # the same calls with the rows read in FP64 by the GPU from the pinned
+    # buffer (no host narrowing), for comparison
+    os.environ["WMD_DROPIN_NARROW"] = "0"
+    wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
+    h2d_dev = wmd.dropin_h2d_bytes()
+    dev_t = []
+    for _ in range(max(2, a.e2e_steps // 2)):
+        t0 = time.perf_counter()
+        wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
+        dev_t.append(time.perf_counter() - t0)
+    del os.environ["WMD_DROPIN_NARROW"]
+    dev_read_value = n_total * len(dev_t) / sum(dev_t)
     e2e_value = n_total * a.e2e_steps / float(e2e_tot.item())
     e2e_pcie_gbs = h2d * a.e2e_steps / float(e2e_tot.item()) / 1e9
     res_value = n_total * a.e2e_steps / float(res_tot.item())
@@ -975,6 +992,13 @@ def ours(a, rank, world, local):
                                     "embeddings split into TF32 high + low "
                                     "parts, three products; FP32 iterations, "
                                     "FP64 final reduction)") if a.cdist == "tf32x3" else
+                                   ("single-source plain Sinkhorn WMD (FP32-"
+                                    "accurate cost panel on tcgen05: resident "
+                                    "split-FP16 embeddings, each row scaled by "
+                                    "a power of two, FP16 high part + remainder "
+                                    "scaled by 2^11, three products; FP32 "
+                                    "iterations, FP64 final reduction)")
+                                   if a.cdist == "f16x3" else
                                    (f"single-source Sinkhorn WMD, {a.cdist.upper()} "
                                     "tensor-core cost panel with FP32 near-pair "
                                     "recompute, FP32 iterations, FP64 final "
@@ -991,10 +1015,17 @@ def ours(a, rank, world, local):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "h2d_input_bytes": h2d_full,
                     "api": ("wmd_sinkhorn_fused_csc (drop-in, pinned host "
-                            "buffers: the GPU reads only the embedding rows of "
-                            "words in the targets or the source; FP32-accurate "
+                            "buffers: only the embedding rows of words in the "
+                            "targets or the source move, narrowed to FP32 by "
+                            f"the host threads ({host_cores()}) and copied in "
+                            "chunks overlapping the conversion; FP32-accurate "
                             "split-TF32 tcgen05 cost panel)"),
                     "h2d_gbs": e2e_pcie_gbs,
+                    "device_read_value": dev_read_value,
+                    "device_read_h2d_bytes_per_step": h2d_dev,
+                    "device_read": ("the same call with WMD_DROPIN_NARROW=0: the "
+                                    "GPU reads the FP64 rows from the pinned "
+                                    "buffer itself"),
                     "resident_corpus_value": res_value,
                     "resident_corpus_h2d_bytes_per_step": p.V * 8,
                     "max_rel_err_vs_oracle": e2e_err},

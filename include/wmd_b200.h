@@ -141,7 +141,16 @@ typedef enum wmd_cdist_mode {
    * lo*hi) accumulated in FP32: FP32-accurate, near pairs recomputed as in
    * WMD_CDIST_FP32.  Widths d that are not a multiple of 4 (or too wide for
    * the tile) use the FP32 CUDA-core panel instead. */
-  WMD_CDIST_TF32X3 = 3
+  WMD_CDIST_TF32X3 = 3,
+  /* tcgen05 tensor cores on a resident split-FP16 copy of the embeddings
+   * (built from the FP32 embeddings on first use, 4*d + 16 bytes per word):
+   * each row scaled by a power of two, an FP16 high part and its remainder
+   * scaled by 2^11 in FP16, three products (hi*hi + 2^-11 (hi*lo + lo*hi))
+   * accumulated in FP32: FP32-accurate like WMD_CDIST_TF32X3, read by TMA
+   * with no in-kernel conversion.  Single-source queries (wmd_query_dense*)
+   * only; batches and widths the tile cannot hold run the WMD_CDIST_TF32X3
+   * form. */
+  WMD_CDIST_F16X3 = 4
 } wmd_cdist_mode;
 
 wmd_status wmd_create(wmd_handle** out, int device);

@@ -301,7 +301,9 @@ class Engine:
     def set_cdist_mode(self, mode: str):
         """Cost panel: "fp32" (CUDA cores, the default), "tf32x3" (tcgen05
         tensor cores on the FP32 embeddings split into TF32 high + low
-        parts: FP32-accurate), "fp16" / "bf16" (16-bit operands)."""
+        parts: FP32-accurate), "f16x3" (tcgen05 on a resident split-FP16
+        copy: FP32-accurate, single-source queries; batches use the tf32x3
+        form), "fp16" / "bf16" (16-bit operands)."""
         check(lib().wmd_set_cdist_mode(self._h, CDIST_MODES[mode]))
 
     def set_relaxation(self, omega: float = 1.0):

@@ -23,7 +23,7 @@ STATUS = {
     6: "WMD_ERR_UNSUPPORTED", 7: "WMD_ERR_DEVICE_TIMEOUT",
 }
 
-CDIST_MODES = {"fp32": 0, "bf16": 1, "fp16": 2, "tf32x3": 3}
+CDIST_MODES = {"fp32": 0, "bf16": 1, "fp16": 2, "tf32x3": 3, "f16x3": 4}
 
 
 class WMDError(RuntimeError):

@@ -25,7 +25,7 @@ LIB = os.path.join(HERE, "libwmd_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-    "-Xcompiler", "-fPIC,-O3,-Wall",
+    "-Xcompiler", "-fPIC,-O3,-Wall,-fopenmp",
     "-I" + INCLUDE, "-I" + CSRC,
 ]
 
@@ -76,7 +76,8 @@ def build(force: bool = False, verbose: bool = False,
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose, extra), _sources()))
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC"]
+    cmd = [nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC,-fopenmp",
+                                                           "-lgomp"]
     if verbose:
         print(" ".join(cmd), flush=True)
     p = subprocess.run(cmd, capture_output=True, text=True)

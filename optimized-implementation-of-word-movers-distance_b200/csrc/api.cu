@@ -12,6 +12,8 @@
 #include <random>
 #include <vector>
 
+#include <omp.h>
+
 #include <cuda.h>
 
 #include "wmd_b200.h"
@@ -40,6 +42,31 @@ wmd_status fail_cuda(cudaError_t e, const char* what) {
     cudaError_t e_ = (call);                              \
     if (e_ != cudaSuccess) return fail_cuda(e_, #call);   \
   } while (0)
+
+// Grow-only pinned host buffer (staging for host -> device copies that run
+// while the host keeps working).
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  ~HostBuf() { release(); }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    const size_t want = bytes ? bytes : 16;
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e == cudaSuccess) cap = want;
+    else p = nullptr;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
 
 // Grow-only device buffer.
 struct DevBuf {
@@ -95,13 +122,13 @@ struct QueryKey {
   float tol = 0.f;
   float omega = 1.f;
   int prec = -1;
-  const void* bufs[24] = {};  // every device buffer the graph reads or writes
+  const void* bufs[25] = {};  // every device buffer the graph reads or writes
   bool operator==(const QueryKey& o) const {
     if (!(r == o.r && out == o.out && cap == o.cap && expo == o.expo &&
           max_iter == o.max_iter && mode == o.mode && timing == o.timing &&
           epoch == o.epoch && tol == o.tol && omega == o.omega && prec == o.prec))
       return false;
-    for (int i = 0; i < 24; ++i)
+    for (int i = 0; i < 25; ++i)
       if (bufs[i] != o.bufs[i]) return false;
     return true;
   }
@@ -133,10 +160,20 @@ struct wmd_handle {
   // embeddings
   DevBuf E32, nE, E64_stage, E16;
   DevBuf need, need_count;  // needed-rows upload of the drop-in calls
+  // Drop-in rows narrowed to FP32 on the host: pinned staging [slot[V] |
+  // rows], their device copies, and the host marks / ids of needed words.
+  HostBuf hstage;
+  DevBuf rows32, slot_dev;
+  std::vector<unsigned char> hmark;
+  std::vector<uint32_t> hids;
   uint64_t dropin_h2d = 0;  // bytes the last drop-in call moved host -> device
   uint64_t V = 0, d = 0;
   bool have_E = false;
   int e16_fmt = -1;  // format E16 holds (1 bf16, 2 fp16), -1 = stale
+  // Split-FP16 rows of the F16X3 cost panel (tc_split_row_bytes(d) each),
+  // built on first use from E32.
+  DevBuf Ehl;
+  bool ehl_ready = false;
   // targets
   DevBuf col_ptr, ent, order, stage_cp, stage_rows, stage_vals;
   DevBuf edge_words, edge_docs, edge_w, edge_temp;  // edge-list CSC build
@@ -302,6 +339,7 @@ wmd_status set_embeddings(wmd_handle* h, const void* vecs, uint64_t V,
   h->d = d;
   h->have_E = true;
   h->e16_fmt = -1;
+  h->ehl_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
   for (int& x : h->warp_shape) x = -2;
@@ -651,10 +689,22 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
     return fail(WMD_ERR_UNSUPPORTED, "more than 1024 non-zero source words");
   const bool tcm = h->mode == WMD_CDIST_BF16 || h->mode == WMD_CDIST_FP16;
   const bool bf16 = h->mode == WMD_CDIST_BF16;
-  // Split-TF32 form; widths it cannot tile use the FP32 CUDA-core panel.
-  const bool x3 = h->mode == WMD_CDIST_TF32X3 && tc_tile_n_x3(cap, d) != 0;
+  // Split-FP16 form; where it cannot tile, the split-TF32 form; widths
+  // neither tiles use the FP32 CUDA-core panel.
+  const bool h2 = h->mode == WMD_CDIST_F16X3 && tc_tile_n_h2(cap, d) != 0;
+  const bool x3 = !h2 && (h->mode == WMD_CDIST_TF32X3 || h->mode == WMD_CDIST_F16X3) &&
+                  tc_tile_n_x3(cap, d) != 0;
   const int dp = tc_padded_width(d);
+  const size_t rs = tc_split_row_bytes(d);
   int launches = 0;
+  if (h2) {
+    if (!h->ehl_ready) {  // split rows of the embeddings, built once
+      CK(h->Ehl.ensure((size_t)V * rs));
+      launches += launch_to_split16(h->E32.as<float>(), V, d, h->Ehl.p, h->stream);
+      h->ehl_ready = true;
+    }
+    CK(h->sel_S16.ensure((size_t)std::max<uint32_t>(cap, 1) * rs));
+  }
   if (tcm) {
     if (tc_tile_n(cap, d) == 0)
       return fail(WMD_ERR_UNSUPPORTED, "embedding width too large for the tensor-core panel");
@@ -711,15 +761,17 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   auto enqueue = [&](bool capturing, int* nlaunch) -> wmd_status {
     int n = 0;
     CK(record(0, capturing));
+    // (the split form's source rows are whole split rows: rs / 2 halves)
     n += launch_select(r_dev, V, h->E32.as<float>(), h->nE.as<float>(), d, sel,
                        h->err_dev.as<unsigned>(), h->stream,
-                       tcm ? h->E16.p : nullptr, tcm ? h->sel_S16.p : nullptr, dp,
+                       tcm ? h->E16.p : h2 ? h->Ehl.p : nullptr,
+                       tcm || h2 ? h->sel_S16.p : nullptr, h2 ? (int)(rs / 2) : dp,
                        near.count);  // the selection also zeroes the near-pair count
     CK(record(1, capturing));
     if (mrow) CK(cudaMemsetAsync(mrow, 0x7f, (size_t)V * sizeof(float), h->stream));
-    if (tcm || x3) {
-      const int lc = launch_cdist_tc(x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
-                                     h->E16.p, h->sel_S16.p,
+    if (tcm || x3 || h2) {
+      const int lc = launch_cdist_tc(h2 ? TC_F16X3 : x3 ? TC_TF32X3 : bf16 ? TC_BF16 : TC_FP16,
+                                     h2 ? h->Ehl.p : h->E16.p, h->sel_S16.p,
                                      h->E32.as<float>(), h->nE.as<float>(), V, d,
                                      sel, expo, h->K.as<float>(), KMp, ld, near,
                                      h->err_dev.as<unsigned>(), h->sms, h->stream, mrow);
@@ -812,13 +864,13 @@ wmd_status query_device(wmd_handle* h, const double* r_dev, uint32_t cap,
   key.omega = h->omega;
   key.prec = (int)h->prec + (ws ? 2 : 0);
   {
-    const DevBuf* used[24] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
+    const DevBuf* used[25] = {&h->E32, &h->nE, &h->E16, &h->sel_ids, &h->sel_rinv,
                               &h->sel_S, &h->sel_nS, &h->sel_S16, &h->K, &h->KM,
                               &h->near_pairs, &h->sel_chunks, &h->iters, &h->K16,
                               &h->ws_Asrc, &h->ws_u0, &h->vstate, &h->mrow,
                               &h->ws_stats, &h->exact_list, &h->exact_count,
-                              &h->wm_u, &h->wm_x, &h->wm_ent};
-    for (int i = 0; i < 24; ++i) key.bufs[i] = used[i]->p;
+                              &h->wm_u, &h->wm_x, &h->wm_ent, &h->Ehl};
+    for (int i = 0; i < 25; ++i) key.bufs[i] = used[i]->p;
     key.prec += word_major ? 16 : 0;
   }
   if (!h->use_graphs) {
@@ -1204,7 +1256,10 @@ wmd_status query_batch(wmd_handle* h, const uint64_t* src_ptr,
   }
   const bool tcm = h->mode == WMD_CDIST_BF16 || h->mode == WMD_CDIST_FP16;
   const bool bf16 = h->mode == WMD_CDIST_BF16;
-  const bool x3 = h->mode == WMD_CDIST_TF32X3 && tc_tile_n_x3(vr_max, d) != 0;
+  // The split-FP16 mode runs its batches on the split-TF32 form (the same
+  // FP32 accuracy class).
+  const bool x3 = (h->mode == WMD_CDIST_TF32X3 || h->mode == WMD_CDIST_F16X3) &&
+                  tc_tile_n_x3(vr_max, d) != 0;
   const int dp = tc_padded_width(d);
   if (tcm && tc_tile_n(vr_max, d) == 0)
     return fail(WMD_ERR_UNSUPPORTED, "embedding width too large for the tensor-core panel");
@@ -1523,11 +1578,96 @@ wmd_status set_embeddings_needed(wmd_handle* h, const double* vecs_mapped,
   h->d = d;
   h->have_E = true;
   h->e16_fmt = -1;
+  h->ehl_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
   for (int& x : h->warp_shape) x = -2;
   h->graph_epoch++;
   h->last_launches = launches;
+  return WMD_OK;
+}
+
+// Drop-in embeddings narrowed on the host: the words a query can touch (the
+// target words of the resident target set, whose row indices the caller's
+// CSC holds and set_targets_csc has range-checked, and the source words
+// r != 0) are converted FP64 -> FP32 by the host threads into pinned memory,
+// chunk by chunk, each chunk copied to the device while the next one is
+// converted; a kernel then places the rows (and their norms) in E32 and
+// zeroes the rest.  The bus carries 4 bytes per needed entry instead of 8,
+// and the FP32 values are those the device-side conversion gives
+// (round to nearest), so the results are bit-identical to the other paths.
+wmd_status set_embeddings_host_rows(wmd_handle* h, const double* vecs, const double* r,
+                                    uint64_t V, uint64_t d, const uint64_t* row_inds,
+                                    uint64_t nnz, uint64_t* nrows) {
+  if (V > 0x7FFFFFFFull)
+    return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^31-1 words");
+  if (d > 65536) return fail(WMD_ERR_UNSUPPORTED, "embedding width above 65536");
+  if (!h->have_T || h->tV != V)
+    return fail(WMD_ERR_INVALID_ARG, "targets must be set first");
+  // Needed words.
+  h->hmark.assign(V, 0);
+  unsigned char* mark = h->hmark.data();
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < (int64_t)nnz; ++e)
+    __atomic_store_n(&mark[row_inds[e]], (unsigned char)1, __ATOMIC_RELAXED);
+  for (uint64_t w = 0; w < V; ++w)
+    if (r[w] != 0.0) mark[w] = 1;
+  // Pinned layout: slot[V] (int32, the row of each word in the row block or
+  // -1), then the row block at a 256-byte boundary.
+  const size_t slot_bytes = ((size_t)V * 4 + 255) & ~(size_t)255;
+  h->hids.clear();
+  for (uint64_t w = 0; w < V; ++w)
+    if (mark[w]) h->hids.push_back((uint32_t)w);
+  const uint64_t count = h->hids.size();
+  const size_t n = (size_t)V * d;
+  CK(h->E32.ensure(n * sizeof(float)));
+  CK(h->nE.ensure((size_t)V * sizeof(float)));
+  CK(h->r_dev.ensure(V * sizeof(double)));
+  CK(h->slot_dev.ensure((size_t)V * 4));
+  CK(h->rows32.ensure(std::max<size_t>(count, 1) * d * sizeof(float)));
+  CK(h->hstage.ensure(slot_bytes + std::max<size_t>(count, 1) * d * sizeof(float)));
+  int32_t* slot = static_cast<int32_t*>(h->hstage.p);
+  float* rows = reinterpret_cast<float*>(static_cast<char*>(h->hstage.p) + slot_bytes);
+  {
+    int32_t k = 0;
+    for (uint64_t w = 0; w < V; ++w) slot[w] = mark[w] ? k++ : -1;
+  }
+  CK(cudaMemcpyAsync(h->slot_dev.p, slot, (size_t)V * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  // Rows, in chunks of about 8 MB of FP32 (at least 8 chunks when there are
+  // enough rows), so the copies overlap the conversion of later chunks.
+  const uint32_t* ids = h->hids.data();
+  const uint64_t per_chunk =
+      std::max<uint64_t>(1, std::min<uint64_t>((8u << 20) / (d * 4) + 1, (count + 7) / 8));
+  for (uint64_t i0 = 0; i0 < count; i0 += per_chunk) {
+    const uint64_t i1 = std::min(count, i0 + per_chunk);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = (int64_t)i0; i < (int64_t)i1; ++i) {
+      const double* src = vecs + (uint64_t)ids[i] * d;
+      float* dst = rows + (uint64_t)i * d;
+      for (uint64_t k = 0; k < d; ++k) dst[k] = (float)src[k];
+    }
+    CK(cudaMemcpyAsync(h->rows32.as<float>() + i0 * d, rows + i0 * d,
+                       (size_t)(i1 - i0) * d * sizeof(float), cudaMemcpyHostToDevice,
+                       h->stream));
+  }
+  int launches = launch_scatter_rows(h->rows32.as<float>(), h->slot_dev.as<int32_t>(), V, d,
+                                     h->E32.as<float>(), h->nE.as<float>(), h->stream);
+  CK(cudaGetLastError());
+  wmd_status se = update_emax(h, V);
+  if (se) return se;
+  launches += 1;
+  h->V = V;
+  h->d = d;
+  h->have_E = true;
+  h->e16_fmt = -1;
+  h->ehl_ready = false;
+  h->ws_docs_ready = false;
+  for (int& x : h->blk_shape) x = -2;
+  for (int& x : h->warp_shape) x = -2;
+  h->graph_epoch++;
+  h->last_launches = launches;
+  *nrows = count;
   return WMD_OK;
 }
 
@@ -1581,9 +1721,23 @@ wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
   wmd_status s = default_handle(&h);
   if (s) return s;
   const uint64_t csc_bytes = (N + 1) * 8 + c->nnz * 16 + N * 4;  // + order
-  const void* vmap = mapped_host_range(vecs, (size_t)V * d * sizeof(double));
+  // Rows narrowed on the host when there are host threads to convert them
+  // (WMD_DROPIN_NARROW=0 turns this off): half the bus bytes of the FP64
+  // rows.  Otherwise pinned, device-mapped embeddings are read in place.
+  const char* nenv = getenv("WMD_DROPIN_NARROW");
+  const bool narrow = omp_get_max_threads() >= 4 && !(nenv && nenv[0] == '0');
+  const void* vmap =
+      narrow ? nullptr : mapped_host_range(vecs, (size_t)V * d * sizeof(double));
   int le = 0, lt = 0;
-  if (vmap) {
+  uint64_t nrows = 0;
+  if (narrow) {
+    s = set_targets_csc(h, c);
+    if (s) return s;
+    lt = h->last_launches;
+    s = set_embeddings_host_rows(h, vecs, r, V, d, c->row_inds, c->nnz, &nrows);
+    if (s) return s;
+    le = h->last_launches;
+  } else if (vmap) {
     // Pinned, device-mapped embeddings: targets first, then only the rows
     // they (and the source) need are read over the bus.
     s = set_targets_csc(h, c);
@@ -1600,9 +1754,13 @@ wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
     if (s) return s;
     lt = h->last_launches;
   }
-  s = query_host(h, r, expo, max_iter, WMD, vmap != nullptr);
+  s = query_host(h, r, expo, max_iter, WMD, narrow || vmap != nullptr);
   if (s) return s;
   h->last_launches += le + lt;
+  if (narrow) {  // CSC + r + the slot map + the FP32 rows
+    h->dropin_h2d = csc_bytes + V * 8 + V * 4 + nrows * d * 4;
+    return WMD_OK;
+  }
   uint64_t rows = V;
   if (vmap) {
     unsigned long long cnt = 0;
@@ -1691,7 +1849,7 @@ wmd_status wmd_destroy(wmd_handle* h) {
   if (!h) return WMD_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (DevBuf* b : {&h->E32, &h->nE, &h->E64_stage, &h->E16, &h->col_ptr,
+  for (DevBuf* b : {&h->E32, &h->nE, &h->E64_stage, &h->E16, &h->Ehl, &h->col_ptr,
                     &h->ent, &h->order, &h->stage_cp, &h->stage_rows,
                     &h->stage_vals, &h->r_dev, &h->sel_ids, &h->sel_rinv,
                     &h->sel_S, &h->sel_nS, &h->sel_S16, &h->sel_vr,
@@ -1759,6 +1917,7 @@ wmd_status wmd_set_embeddings_bf16(wmd_handle* h, const uint16_t* vecs, uint64_t
   h->d = d;
   h->have_E = true;
   h->e16_fmt = 1;  // E16 holds the BF16 embeddings themselves
+  h->ehl_ready = false;
   h->ws_docs_ready = false;
   for (int& x : h->blk_shape) x = -2;
   for (int& x : h->warp_shape) x = -2;
@@ -1792,7 +1951,7 @@ wmd_status wmd_set_targets_csr(wmd_handle* h, const wmd_csr_double_t* a) {
 wmd_status wmd_set_cdist_mode(wmd_handle* h, wmd_cdist_mode mode) {
   if (!h) return fail(WMD_ERR_INVALID_ARG, "null handle");
   if (mode != WMD_CDIST_FP32 && mode != WMD_CDIST_BF16 && mode != WMD_CDIST_FP16 &&
-      mode != WMD_CDIST_TF32X3)
+      mode != WMD_CDIST_TF32X3 && mode != WMD_CDIST_F16X3)
     return fail(WMD_ERR_INVALID_ARG, "unknown cdist mode");
   h->mode = mode;
   return WMD_OK;

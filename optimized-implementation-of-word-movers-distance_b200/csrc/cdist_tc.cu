@@ -44,6 +44,7 @@
 // results.  Only the FP32 embeddings are read: no 16-bit or split copies are
 // kept in HBM.
 #include <cuda.h>
+#include <cstring>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -70,12 +71,17 @@ constexpr int kTileBytesA = BM * 128;  // 16 KB: 128 rows of 128 bytes
 #endif
 constexpr int kMaxStages = WMD_TC_MAX_STAGES;
 constexpr int kSlots = WMD_TC_X3_SLOTS;
-template <bool X3>
+// H2: the split-FP16 form (kind::f16 on FP16 high and scaled low parts of
+// the embeddings, both read from HBM by TMA: two vocabulary tiles per ring
+// stage, no converter warps).
+template <bool X3, bool H2 = false>
 struct Form {
+  static_assert(!(X3 && H2), "one split form");
   static constexpr int kThreads = X3 ? 448 : 320;   // + 4 converter warps
   static constexpr int kChunk = X3 ? 32 : BK;       // elements per chunk row
-  static constexpr int kMult = X3 ? 2 : 1;          // B buffers (hi, lo)
+  static constexpr int kMult = (X3 || H2) ? 2 : 1;  // B buffers (hi, lo)
   static constexpr int kSlotBytes = X3 ? kSlots * 2 * kTileBytesA : 0;
+  static constexpr int kStageBytes = (H2 ? 2 : 1) * kTileBytesA;  // ring stage
 };
 
 struct Params {
@@ -93,6 +99,11 @@ struct Params {
   // [tiles[y].z, + NT) of source tiles[y].x's panel (grp[]).
   const int4* tiles;
   const GroupSrc* grp;
+  // Split-FP16 form: 1/s of each vocabulary row (esc) and of each source row
+  // (ssc), one FP32 value every sc_stride floats (inside the split rows).
+  const float* esc;
+  const float* ssc;
+  int sc_stride;
   unsigned* err;
   uint64_t V;
   int d, ld, NT, KT, tmem_cols, stages;
@@ -106,23 +117,26 @@ struct Params {
 //                                 rows: one N = 2 NT operand [hi | lo])
 //   barriers full[stages], empty[stages], conv[kSlots], mfree[kSlots],
 //            bfull, bconv, accf[2], acce[2]
-//   tmem address slot, nS copy [NT]
-template <bool X3>
+//   tmem address slot, nS copy [NT] (H2: + source scales [NT])
+// H2: each ring stage holds the high then the low tile (2 x 16 KB), and B
+// per chunk NT high rows then NT low rows, both loaded by TMA.
+template <bool X3, bool H2 = false>
 __host__ __device__ inline size_t smem_fixed_bytes(int NT, int KT) {
-  return 1024 + (size_t)Form<X3>::kSlotBytes +
-         (size_t)KT * NT * 128 * Form<X3>::kMult + (2 * kSlots + 6) * 8 + 16 +
-         (size_t)NT * 4;
+  return 1024 + (size_t)Form<X3, H2>::kSlotBytes +
+         (size_t)KT * NT * 128 * Form<X3, H2>::kMult + (2 * kSlots + 6) * 8 + 16 +
+         (size_t)NT * 4 * (H2 ? 2 : 1);
 }
-template <bool X3>
+template <bool X3, bool H2 = false>
 __host__ __device__ inline size_t smem_bytes(int NT, int KT, int stages) {
-  return smem_fixed_bytes<X3>(NT, KT) + (size_t)stages * (kTileBytesA + 16);
+  return smem_fixed_bytes<X3, H2>(NT, KT) +
+         (size_t)stages * (Form<X3, H2>::kStageBytes + 16);
 }
 // Deepest ring that fits in `budget` bytes (0 if not even two stages fit).
-template <bool X3>
+template <bool X3, bool H2 = false>
 inline int ring_stages(int NT, int KT, size_t budget) {
-  const size_t fixed = smem_fixed_bytes<X3>(NT, KT);
+  const size_t fixed = smem_fixed_bytes<X3, H2>(NT, KT);
   if (fixed >= budget) return 0;
-  int st = (int)((budget - fixed) / (kTileBytesA + 16));
+  int st = (int)((budget - fixed) / (Form<X3, H2>::kStageBytes + 16));
   if (st > kMaxStages) st = kMaxStages;
   return st >= 2 ? st : 0;
 }
@@ -143,20 +157,25 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <bool X3>
-__global__ void __launch_bounds__(Form<X3>::kThreads, 1)
+// tmA2 / tmB2: the low parts of the split-FP16 form (H2; unused otherwise).
+template <bool X3, bool H2 = false>
+__global__ void __launch_bounds__(Form<X3, H2>::kThreads, 1)
 cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
-                const __grid_constant__ CUtensorMap tmB, const Params p,
+                const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ CUtensorMap tmA2,
+                const __grid_constant__ CUtensorMap tmB2, const Params p,
                 const uint32_t idesc, const uint32_t idesc2) {
-  constexpr int MU = Form<X3>::kMult;
-  constexpr int CH = Form<X3>::kChunk;
+  using Fm = Form<X3, H2>;
+  constexpr int MU = Fm::kMult;
+  constexpr int CH = Fm::kChunk;
+  constexpr int SB = Fm::kStageBytes;
   const int ST = p.stages;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* sA = base;
-  unsigned char* sSlot = sA + (size_t)ST * kTileBytesA;  // X3 only
-  unsigned char* sB = sSlot + Form<X3>::kSlotBytes;
+  unsigned char* sSlot = sA + (size_t)ST * SB;  // X3 only
+  unsigned char* sB = sSlot + Fm::kSlotBytes;
   const size_t bbytes = (size_t)p.KT * p.NT * 128;  // bytes TMA loads
   const size_t bchunk = (size_t)MU * p.NT * 128;    // smem per B chunk
   const int accw = MU * p.NT;                       // accumulator columns
@@ -172,6 +191,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
   uint64_t* acce = accf + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
   float* nS_s = reinterpret_cast<float*>(tmem_slot + 4);
+  float* ss_s = nS_s + p.NT;  // H2: source row scales
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // This CTA's N-tile: its first stacked source row (TMA, norms, near-pair
@@ -219,6 +239,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
   }
   for (int c = threadIdx.x; c < p.NT; c += blockDim.x) {
     nS_s[c] = col0 + c < vr ? p.nS[n0 + c] : 0.f;
+    if constexpr (H2) ss_s[c] = col0 + c < vr ? p.ssc[(size_t)(n0 + c) * p.sc_stride] : 0.f;
   }
   fence_before();
   __syncthreads();
@@ -229,9 +250,12 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
     if (warp == 0) {
       if (lane == 0) {
         // ---- TMA producer ----
-        mbar_expect_tx(bfull, (uint32_t)bbytes);
-        for (int q = 0; q < p.KT; ++q)
+        mbar_expect_tx(bfull, (uint32_t)(bbytes * (H2 ? 2 : 1)));
+        for (int q = 0; q < p.KT; ++q) {
           tma_load_2d(sB + (size_t)q * bchunk, &tmB, bfull, q * CH, n0);
+          if constexpr (H2)
+            tma_load_2d(sB + (size_t)q * bchunk + (size_t)p.NT * 128, &tmB2, bfull, q * CH, n0);
+        }
         uint32_t it = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -241,9 +265,11 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
               ok = false;
               break;
             }
-            mbar_expect_tx(&full[s], kTileBytesA);
-            tma_load_2d(sA + (size_t)s * kTileBytesA, &tmA, &full[s], q * CH,
-                        tile * BM);
+            mbar_expect_tx(&full[s], SB);
+            tma_load_2d(sA + (size_t)s * SB, &tmA, &full[s], q * CH, tile * BM);
+            if constexpr (H2)
+              tma_load_2d(sA + (size_t)s * SB + kTileBytesA, &tmA2, &full[s], q * CH,
+                          tile * BM);
           }
         }
       }
@@ -286,11 +312,25 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                 break;
               }
               fence_after();
-              const uint32_t a0 = smem_u32(sA + (size_t)s * kTileBytesA);
+              const uint32_t a0 = smem_u32(sA + (size_t)s * SB);
+              if constexpr (H2) {
+                // Columns [0, NT) accumulate hi.hi, columns [NT, 2 NT) the
+                // cross terms (both scaled by 2^11): hi.[hi | lo'] as one
+                // N = 2 NT product, then lo'.hi into the second half.
 #pragma unroll
-              for (int kk = 0; kk < 4; ++kk)
-                mma_f16(dt, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
-                        idesc, (q > 0 || kk > 0) ? 1u : 0u);
+                for (int kk = 0; kk < 4; ++kk) {
+                  const uint64_t bd = sw128_desc(b0 + kk * 32);
+                  mma_f16(dt, sw128_desc(a0 + kk * 32), bd, idesc2,
+                          (q > 0 || kk > 0) ? 1u : 0u);
+                  mma_f16(dt + (uint32_t)p.NT, sw128_desc(a0 + kTileBytesA + kk * 32), bd,
+                          idesc, 1u);
+                }
+              } else {
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                  mma_f16(dt, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
+                          idesc, (q > 0 || kk > 0) ? 1u : 0u);
+              }
               mma_commit(&empty[s]);  // stage free once these MMAs retire
             }
           }
@@ -328,7 +368,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             break;
           }
           constexpr int kPer = kTileBytesA / 16 / 128;  // float4 per thread
-          const float4* raw = reinterpret_cast<const float4*>(sA + (size_t)s * kTileBytesA);
+          const float4* raw = reinterpret_cast<const float4*>(sA + (size_t)s * SB);
           float4 x[kPer];
 #pragma unroll
           for (int k = 0; k < kPer; ++k) x[k] = raw[c + 128 * k];
@@ -368,6 +408,7 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
         const uint64_t w = (uint64_t)tile * BM + row;
         const bool wok = w < p.V;
         const float ne = wok ? p.nE[w] : 0.f;  // issued before the wait
+        const float sw = H2 && wok ? p.esc[w * (uint64_t)p.sc_stride] : 1.f;
         float mmin = __int_as_float(0x7f7f7f7f);  // row-scaled form
         if (!mbar_wait(&accf[b], tph, p.err)) break;
         fence_after();
@@ -380,6 +421,12 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             tmem_ld16(ta + p.NT, acc2);
 #pragma unroll
             for (int j = 0; j < 16; ++j) acc[j] += acc2[j];
+          } else if constexpr (H2) {
+            float acc2[16];
+            tmem_ld16(ta + p.NT, acc2);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              acc[j] = fmaf(acc2[j], 0x1p-11f, acc[j]) * (sw * ss_s[c0 + j]);
           }
           if (!wok) continue;
           // Straight-line over the 16 entries (no branch inside), so their
@@ -488,6 +535,43 @@ __global__ void to16_kernel(const float* __restrict__ src, uint64_t rows, int d,
     dst[idx] = __float2half_rn(v);
 }
 
+// FP32 [V][d] -> split-FP16 rows of the F16X3 panel, one warp per row.
+// Row w is scaled by s = 2^(14 - e), e the binary exponent of max_k |E_wk|
+// (max < 2^e), so the largest scaled entry lies in [2^13, 2^14); then
+//   hi = fp16(x s),  lo = fp16((x s - hi) 2^11)      (x s - hi is exact)
+// and the row is stored as [hi: dp halves][lo: dp halves][1/s: FP32][pad to
+// 16 bytes], 4 dp + 16 bytes.  hi + 2^-11 lo carries 22 significant bits of
+// x s (the scaled remainder keeps lo clear of FP16's subnormal range), so
+// hi.hi + 2^-11 (hi.lo + lo.hi) is a dot product to about FP32 accuracy,
+// like the split-TF32 form.  A row of zeros keeps s = 1.
+__global__ void to_split16_kernel(const float* __restrict__ src, uint64_t rows, int d,
+                                  int dp, unsigned char* __restrict__ dst) {
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= rows) return;
+  const float* e = src + w * (uint64_t)d;
+  float m = 0.f;
+  for (int k = lane; k < d; k += 32) m = fmaxf(m, fabsf(e[k]));
+#pragma unroll
+  for (int off = 16; off; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  int ex = 0;
+  if (m > 0.f) frexpf(m, &ex);
+  const int sh = max(-126, min(126, 14 - ex));
+  const float sc = ldexpf(1.f, sh);
+  __half* hrow = reinterpret_cast<__half*>(dst + w * (uint64_t)(4 * dp + 16));
+  __half* lrow = hrow + dp;
+  for (int k = lane; k < dp; k += 32) {
+    const float x = k < d ? e[k] * sc : 0.f;
+    const __half h = __float2half_rn(x);
+    hrow[k] = h;
+    lrow[k] = __float2half_rn((x - __half2float(h)) * 2048.f);
+  }
+  if (lane < 4) {
+    float* tail = reinterpret_cast<float*>(lrow + dp);
+    tail[lane] = lane == 0 ? ldexpf(1.f, -sh) : 0.f;
+  }
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------------------
@@ -514,13 +598,14 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+// stride: bytes between rows (0: dense rows of inner elements).
 bool make_map(CUtensorMap* tm, const void* ptr, CUtensorMapDataType dt,
               int esize, uint64_t inner, uint64_t rows, uint32_t box_inner,
-              uint32_t box_rows) {
+              uint32_t box_rows, uint64_t stride = 0) {
   EncodeTiledFn f = encode_fn();
   if (!f) return false;
   const cuuint64_t gdim[2] = {inner, rows};
-  const cuuint64_t gstride[1] = {inner * (uint64_t)esize};
+  const cuuint64_t gstride[1] = {stride ? stride : inner * (uint64_t)esize};
   const cuuint32_t box[2] = {box_inner, box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return f(tm, dt, 2, const_cast<void*>(ptr), gdim, gstride, box, estr,
@@ -529,13 +614,13 @@ bool make_map(CUtensorMap* tm, const void* ptr, CUtensorMapDataType dt,
            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <bool X3>
+template <bool X3, bool H2 = false>
 void set_smem_attr() {
   static bool done[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && !done[dev]) {
-    cudaFuncSetAttribute(tc::cdist_tc_kernel<X3>,
+    cudaFuncSetAttribute(tc::cdist_tc_kernel<X3, H2>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     done[dev] = true;
   }
@@ -569,6 +654,27 @@ int tc_tile_n_x3(uint32_t cap, uint64_t d) {
   return nt;
 }
 
+int tc_tile_n_h2(uint32_t cap, uint64_t d) {
+  const int KT = (int)((tc_padded_width(d) + tc::BK - 1) / tc::BK);
+  int nt = (int)(((cap ? cap : 1) + 15) & ~15u);
+  if (nt > 64) nt = 64;
+  while (nt > 16 && tc::ring_stages<false, true>(nt, KT, kSmemBudget) < kMinStages) nt -= 16;
+  if (tc::ring_stages<false, true>(nt, KT, kSmemBudget) < kMinStages) return 0;
+  return nt;
+}
+
+size_t tc_split_row_bytes(uint64_t d) { return 4 * (size_t)tc_padded_width(d) + 16; }
+
+int launch_to_split16(const float* E32, uint64_t rows, uint64_t d, void* Esplit,
+                      cudaStream_t st) {
+  if (rows == 0) return 0;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((rows * 32 + threads - 1) / threads);
+  tc::to_split16_kernel<<<blocks, threads, 0, st>>>(E32, rows, (int)d, tc_padded_width(d),
+                                                     static_cast<unsigned char*>(Esplit));
+  return 1;
+}
+
 int launch_to16(const float* E32, uint64_t rows, uint64_t d, void* E16,
                 bool bf16, cudaStream_t st) {
   const int dp = tc_padded_width(d);
@@ -592,11 +698,31 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
                     const NearList& near, unsigned* err, int num_sms,
                     cudaStream_t st, float* mrow, const StackedPanels* grp) {
   const bool x3 = form == TC_TF32X3;
+  const bool h2 = form == TC_F16X3;
   // stacked group: s.cap is the number of stacked source rows
   const uint64_t rows_b = s.cap ? s.cap : 1;
   int NT, KT;
-  CUtensorMap tmA, tmB;
-  if (x3) {
+  CUtensorMap tmA, tmB, tmA2, tmB2;
+  memset(&tmA2, 0, sizeof(tmA2));
+  memset(&tmB2, 0, sizeof(tmB2));
+  const int dps = tc_padded_width(d);
+  const uint64_t rs = tc_split_row_bytes(d);
+  if (h2) {
+    if (grp) return -1;  // single-source panels only
+    NT = tc_tile_n_h2(s.cap, d);
+    if (NT == 0) return -1;
+    KT = (dps + tc::BK - 1) / tc::BK;
+    // High and low halves of the split rows (row stride rs): two maps per
+    // operand over the same rows; columns past dp read as zeros.
+    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const unsigned char* e = static_cast<const unsigned char*>(E16);
+    const unsigned char* sp = static_cast<const unsigned char*>(S16);
+    if (!make_map(&tmA, e, dt, 2, (uint64_t)dps, V, tc::BK, tc::BM, rs) ||
+        !make_map(&tmA2, e + 2 * dps, dt, 2, (uint64_t)dps, V, tc::BK, tc::BM, rs) ||
+        !make_map(&tmB, sp, dt, 2, (uint64_t)dps, rows_b, tc::BK, (uint32_t)NT, rs) ||
+        !make_map(&tmB2, sp + 2 * dps, dt, 2, (uint64_t)dps, rows_b, tc::BK, (uint32_t)NT, rs))
+      return -1;
+  } else if (x3) {
     NT = grp ? grp->nt : tc_tile_n_x3(s.cap, d);
     if (NT == 0) return -1;
     KT = (int)((d + 31) / 32);
@@ -623,6 +749,11 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
   tc::Params p;
   p.tiles = grp ? grp->tiles : nullptr;
   p.grp = grp ? grp->src : nullptr;
+  p.esc = h2 ? reinterpret_cast<const float*>(static_cast<const unsigned char*>(E16) + 4 * dps)
+             : nullptr;
+  p.ssc = h2 ? reinterpret_cast<const float*>(static_cast<const unsigned char*>(S16) + 4 * dps)
+             : nullptr;
+  p.sc_stride = (int)(rs / 4);
   p.E32 = E32;
   p.nE = nE;
   p.S32 = s.S;
@@ -639,11 +770,12 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
   p.NT = NT;
   p.KT = KT;
   int cols = 32;
-  while (cols < (x3 ? 4 : 2) * NT) cols <<= 1;  // two accumulators
+  while (cols < (x3 || h2 ? 4 : 2) * NT) cols <<= 1;  // two accumulators
   p.tmem_cols = cols;
   p.expo = expo;
-  p.stages = x3 ? tc::ring_stages<true>(NT, KT, kSmemBudget)
-                : tc::ring_stages<false>(NT, KT, kSmemBudget);
+  p.stages = x3   ? tc::ring_stages<true>(NT, KT, kSmemBudget)
+             : h2 ? tc::ring_stages<false, true>(NT, KT, kSmemBudget)
+                  : tc::ring_stages<false>(NT, KT, kSmemBudget);
   if (p.stages < kMinStages) return -1;
   const int ntiles = (int)((V + tc::BM - 1) / tc::BM);
   int gx = num_sms / ntn;
@@ -657,13 +789,20 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
     const uint32_t idesc2 = tc::make_idesc(2, BM_ROWS, 2 * NT);
     tc::cdist_tc_kernel<true><<<grid, tc::Form<true>::kThreads,
                                 tc::smem_bytes<true>(NT, KT, p.stages), st>>>(
-        tmA, tmB, p, idesc, idesc2);
+        tmA, tmB, tmA2, tmB2, p, idesc, idesc2);
+  } else if (h2) {
+    set_smem_attr<false, true>();
+    const uint32_t idesc = tc::make_idesc(0, BM_ROWS, NT);
+    const uint32_t idesc2 = tc::make_idesc(0, BM_ROWS, 2 * NT);
+    tc::cdist_tc_kernel<false, true><<<grid, tc::Form<false, true>::kThreads,
+                                       tc::smem_bytes<false, true>(NT, KT, p.stages), st>>>(
+        tmA, tmB, tmA2, tmB2, p, idesc, idesc2);
   } else {
     set_smem_attr<false>();
     const uint32_t idesc = tc::make_idesc(form == TC_BF16 ? 1 : 0, BM_ROWS, NT);
     tc::cdist_tc_kernel<false><<<grid, tc::Form<false>::kThreads,
                                  tc::smem_bytes<false>(NT, KT, p.stages), st>>>(
-        tmA, tmB, p, idesc, idesc);
+        tmA, tmB, tmA2, tmB2, p, idesc, idesc);
   }
   return 1;
 }

@@ -167,6 +167,45 @@ int launch_gather_needed_f64(const double* src_mapped, uint64_t V, uint64_t d,
   return 2;
 }
 
+// Needed rows narrowed to FP32 on the host (drop-in calls, staged through
+// pinned memory by api.cu): rows32 holds the needed rows in ascending word order,
+// slot[w] the row of word w in rows32 or -1.  Writes E32 and the norms
+// exactly as gather_convert_f64_kernel does (the same per-lane order of the
+// FP64 norm sums), zeroes the rows nobody needs.
+__global__ void scatter_rows_kernel(const float* __restrict__ rows32,
+                                    const int32_t* __restrict__ slot, uint64_t V,
+                                    uint64_t d, float* __restrict__ E32,
+                                    float* __restrict__ nE) {
+  const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= V) return;
+  float* o = E32 + row * d;
+  const int32_t sl = slot[row];
+  if (sl < 0) {
+    for (uint64_t k = lane; k < d; k += 32) o[k] = 0.f;
+    if (lane == 0) nE[row] = 0.f;
+    return;
+  }
+  const float* s = rows32 + (uint64_t)sl * d;
+  double acc = 0.0;
+  for (uint64_t k = lane; k < d; k += 32) {
+    const float f = s[k];
+    o[k] = f;
+    acc += (double)f * (double)f;
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) nE[row] = (float)acc;
+}
+
+int launch_scatter_rows(const float* rows32, const int32_t* slot, uint64_t V, uint64_t d,
+                        float* E32, float* nE, cudaStream_t st) {
+  const int threads = 256;
+  scatter_rows_kernel<<<(unsigned)((V * 32 + threads - 1) / threads), threads, 0, st>>>(
+      rows32, slot, V, d, E32, nE);
+  return 1;
+}
+
 // ---------------------------------------------------------------------------
 // Targets: validate a CSC triple and pack it for the solver.  The checks are
 // those of the reference driver's MTX reader (sinkhorn_wmd_fused.cpp:474-478):
@@ -247,6 +286,20 @@ __device__ __forceinline__ unsigned block_sum_u32(unsigned v, unsigned* red) {
 // Copy of one embedding row by a warp.  For d <= 512 every lane issues all
 // its loads before its stores (one memory round trip for the row instead of
 // one per 32 elements: the rows are cold in L2 when a query starts).
+// A row of dp 16-bit values, one warp: 16-byte pieces when dp is a multiple
+// of 8 (rows then start on 16-byte boundaries), else element by element.
+__device__ __forceinline__ void copy_row16(const unsigned short* __restrict__ src,
+                                           unsigned short* __restrict__ dst, int dp,
+                                           int lane) {
+  if (dp % 8 == 0) {
+    const uint4* s4 = reinterpret_cast<const uint4*>(src);
+    uint4* d4 = reinterpret_cast<uint4*>(dst);
+    for (int k = lane; k < dp / 8; k += 32) d4[k] = __ldg(s4 + k);
+  } else {
+    for (int k = lane; k < dp; k += 32) dst[k] = src[k];
+  }
+}
+
 __device__ __forceinline__ void copy_row(const float* __restrict__ src,
                                          float* __restrict__ dst, uint64_t d,
                                          int lane) {
@@ -369,11 +422,8 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     float* dst = S + (uint64_t)pos * d;
     copy_row(src, dst, d, lane);
     if (lane == 0) nS[pos] = nE[id];
-    if (S16) {  // 16-bit copy for the tensor-core cost panel
-      const unsigned short* s16 = E16 + id * (uint64_t)dp;
-      unsigned short* d16 = S16 + (uint64_t)pos * dp;
-      for (int k = lane; k < dp; k += 32) d16[k] = s16[k];
-    }
+    if (S16)  // 16-bit (or split) row for the tensor-core cost panel
+      copy_row16(E16 + id * (uint64_t)dp, S16 + (uint64_t)pos * dp, dp, lane);
   }
 }
 
@@ -419,11 +469,7 @@ __global__ void gather_sources_kernel(const uint32_t* __restrict__ ids, int coun
   float* dst = S + (uint64_t)w * d;
   copy_row(src, dst, d, lane);
   if (lane == 0) nS[w] = nE[id];
-  if (S16) {
-    const unsigned short* s16 = E16 + id * (uint64_t)dp;
-    unsigned short* d16 = S16 + (uint64_t)w * dp;
-    for (int k = lane; k < dp; k += 32) d16[k] = s16[k];
-  }
+  if (S16) copy_row16(E16 + id * (uint64_t)dp, S16 + (uint64_t)w * dp, dp, lane);
 }
 
 int launch_gather_sources(const uint32_t* ids, int count, const float* E32,

@@ -21,7 +21,7 @@
 // `omp atomic`, fused:284), no global u/x traffic and no per-iteration
 // launches.  The document's K rows are gathered once from the L2-resident
 // panel and re-used by every iteration from the fastest place they fit:
-// the first one or two rounds of rows stay in registers, the next ones are
+// the first one to three rounds of rows stay in registers, the next ones are
 // staged in shared memory, any remainder is re-gathered from L2.  A
 // document's word ids and weights are staged first (independent loads), so
 // every row gather is issued from on-chip addresses without a dependent L2
@@ -32,8 +32,9 @@
 // ("a round") are in flight per warp.  For v_r <= 32 (LPW = 1) each lane holds
 // a whole K row: the dot product K_w . u needs no shuffle and the 64 FMAs per
 // word run as 32 packed FFMA2.  The x accumulators of the word slots are
-// combined once per iteration through a swizzled 4 KB shared-memory
-// transpose, after which every lane recomputes u for its dimensions.
+// combined once per iteration through a 4.5 KB shared-memory transpose
+// (rows padded to 36 floats), after which every lane recomputes u for its
+// dimensions.
 #include "wmd_internal.cuh"
 
 namespace wmd {
@@ -41,9 +42,11 @@ namespace wmd {
 // Launch shape (warps per CTA, CTAs per SM) and arithmetic form: build-time
 // tuning knobs, the defaults being the measured best on B200.
 // Wide sources (LPW > 1): 4 warps x 2 CTAs per SM, two staged rounds in
-// flight.  v_r <= 32 (LPW = 1): one-warp CTAs, eight per SM, one round in
-// flight -- the same occupancy, measured 6 % faster there and 12-27 % slower
-// for the wide instantiations.
+// flight.  v_r <= 32 (LPW = 1): one-warp CTAs, eight per SM, two staged
+// rounds in flight and three rounds of rows in registers (eight rounds on
+// chip: every document of up to 256 words without an L2 re-gather) -- the
+// same occupancy; one-warp CTAs measured 6 % faster there and 12-27 %
+// slower for the wide instantiations.
 #ifndef WMD_SOLVE_WARPS
 #define WMD_SOLVE_WARPS 4
 #endif
@@ -57,25 +60,22 @@ namespace wmd {
 #define WMD_SOLVE_CTAS_PER_SM_1 8
 #endif
 #ifndef WMD_SOLVE_UNROLL_1
-#define WMD_SOLVE_UNROLL_1 1
+#define WMD_SOLVE_UNROLL_1 2
 #endif
 #ifndef WMD_SOLVE_PACKED_FMA
 #define WMD_SOLVE_PACKED_FMA 1
 #endif
-#ifndef WMD_SOLVE_REG_ROUNDS  // rounds of K rows kept in registers, LPW <= 4
+#ifndef WMD_SOLVE_REG_ROUNDS  // rounds of K rows kept in registers, 2 <= LPW <= 4
 #define WMD_SOLVE_REG_ROUNDS 2
+#endif
+#ifndef WMD_SOLVE_REG_ROUNDS_1  // the same for LPW = 1 (v_r <= 32), unrelaxed
+#define WMD_SOLVE_REG_ROUNDS_1 3
 #endif
 #ifndef WMD_SOLVE_UNROLL  // staged rounds in flight per step
 #define WMD_SOLVE_UNROLL 2
 #endif
 #ifndef WMD_SOLVE_DOT_CHAINS  // independent accumulators per dot product
 #define WMD_SOLVE_DOT_CHAINS 2
-#endif
-// Staged-row layout: 0 = 32-float row slices XOR-swizzled per lane (no
-// padding; every load computes its chunk address), 1 = slices padded to 36
-// floats (conflict-free at compile-time offsets, 12.5 % more shared memory).
-#ifndef WMD_SOLVE_PAD
-#define WMD_SOLVE_PAD 0
 #endif
 
 namespace {
@@ -88,9 +88,11 @@ struct SolveCfg {
   static constexpr int kUnroll = LPW == 1 ? WMD_SOLVE_UNROLL_1 : WMD_SOLVE_UNROLL;
 };
 
+// 16-byte copy global -> shared through L1 (.ca): a lane stages a row in
+// 16-byte pieces, so the second half of each 32-byte sector hits L1.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem)
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
@@ -101,6 +103,15 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
   return __ffma2_rn(a, b, c);
 #else
   return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+
+// Packed add (FADD2): each half rounded as the scalar add.
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+#if WMD_SOLVE_PACKED_FMA
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
 #endif
 }
 
@@ -121,17 +132,21 @@ __device__ __forceinline__ void ones_row(Row& r) {
 }
 }  // namespace
 
-template <int LPW>
+template <int LPW, bool RLX = false>
 struct SolveShape {
   static constexpr int WPS = 32 / LPW;  // words per round
   static constexpr int RL = 32 * LPW;   // padded row length (floats)
   static constexpr int NCH = RL / 4;    // float4 chunks per padded row
-  // float4 slots per 32-float slice of a staged row (8 chunks, + 1 pad)
-  static constexpr int SLC = WMD_SOLVE_PAD ? 9 : 8;
-  static constexpr int SROW = LPW * SLC;  // float4 slots per staged row
+  static constexpr int SROW = NCH;  // float4 slots per staged row
+  // Row pitch (floats) of the 32 x 32 transpose buffer: 36 puts the rows of
+  // the 8 lanes of a 16-byte shared-memory phase on distinct bank groups
+  // with no address arithmetic per access.
+  static constexpr int RP = 36;
   // Rounds of K rows kept in registers (fewer when the per-lane dimension
-  // arrays of wide sources already use the register budget).
-  static constexpr int RR = LPW <= 4 ? WMD_SOLVE_REG_ROUNDS : 1;
+  // arrays of wide sources, or the relaxation state, already use the
+  // register budget).
+  static constexpr int RR = LPW == 1 ? (RLX ? 2 : WMD_SOLVE_REG_ROUNDS_1)
+                                     : (LPW <= 4 ? WMD_SOLVE_REG_ROUNDS : 1);
   static_assert(LPW >= 1 && LPW <= 32 && (LPW & (LPW - 1)) == 0, "LPW");
   // Per-warp shared memory: staged rows (whole rounds), staged entries
   // {word id, weight} of the register and staged rounds, 32x32 transpose
@@ -143,7 +158,7 @@ struct SolveShape {
     return (size_t)srounds * WPS * SROW * 16;
   }
   static __host__ __device__ size_t warp_bytes(int srounds) {
-    return staged_bytes(srounds) + entries_bytes(srounds) + 32 * 32 * 4 + RL * 4;
+    return staged_bytes(srounds) + entries_bytes(srounds) + 32 * RP * 4 + RL * 4;
   }
 };
 
@@ -166,7 +181,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
              const float* __restrict__ u0, int64_t ldu, float omega,
              float* __restrict__ vstate, const float* __restrict__ mrow,
              double* __restrict__ out, const GroupSrc* __restrict__ grp, int nsrc) {
-  using Sh = SolveShape<LPW>;
+  using Sh = SolveShape<LPW, RLX>;
   constexpr int WPS = Sh::WPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -177,7 +192,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
   uint2* sE = reinterpret_cast<uint2*>(wbase + Sh::staged_bytes(srounds));
   float* red = reinterpret_cast<float*>(wbase + Sh::staged_bytes(srounds) +
                                         Sh::entries_bytes(srounds));
-  float* ubuf = red + 32 * 32;
+  float* ubuf = red + 32 * Sh::RP;
   // GRP: the current source's arguments, one copy per warp in shared
   // memory, read where they are used instead of being held in registers for
   // the whole document loop (which spilled the wide instantiations).
@@ -196,11 +211,13 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
     if constexpr (GRP) return gs.mrow;
     else return mrow;
   };
-  // Staged row s holds logical chunk 8q'+t at 8q' + (t ^ ((s*LPW + q') & 7)).
-  // For the lane that reads it s*LPW + q = 32*round + lane, so the key is
-  // lane & 7: constant per lane, and the 8 lanes of a shared-memory phase hit
-  // 8 distinct bank groups.
-  const int key = lane & 7;
+  // Staged rounds are chunk-major: chunk t (dimensions 4t..4t+3 of the
+  // lane's slice) of the row lane L holds in staged round s sits at float4
+  // s * 256 + t * 32 + L.  A lane stages and reads only its own rows; the 8
+  // lanes of a 16-byte shared-memory phase touch 8 consecutive slots (no
+  // bank conflict), and every load is at an immediate offset from the
+  // lane's base sK + L (rounds 4 KB apart, chunks 512 bytes apart).
+  const float4* const sKl = sK + lane;
 
   // Dimensions this lane finalises after the transpose: 32*qq + own, with
   // own = 2 (lane % 16) + lane / 16 when the slot sums run in pairs
@@ -309,18 +326,24 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
         ones_row(reg[t]);
       }
     }
-    // Staged rows: rounds [rr, rr + sr), padded with ones rows to whole rounds.
-    for (int c = lane; c < sr * WPS * Sh::NCH; c += 32) {
-      const int s = c / Sh::NCH, lc = c % Sh::NCH;
-      const int k = rr * WPS + s;
-      float4* dst = WMD_SOLVE_PAD
-                        ? sK + (size_t)(s * LPW + (lc >> 3)) * Sh::SLC + (lc & 7)
-                        : sK + (size_t)s * Sh::NCH + 8 * (lc >> 3) +
-                              ((lc & 7) ^ ((s * LPW + (lc >> 3)) & 7));
-      if (k < n && lc < ldc)
-        cp_async16(dst, Kd + (size_t)sE[k].x * ld + 4 * lc);
-      else
-        *dst = k < n ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(1.f, 1.f, 1.f, 1.f);
+    // Staged rows: rounds [rr, rr + sr), each lane its own row slice, padded
+    // with ones rows to whole rounds; chunks past the panel width are zero.
+    for (int r = 0; r < sr; ++r) {
+      const int k = (rr + r) * WPS + g;
+      float4* dst = sK + r * (WPS * Sh::NCH) + lane;
+      if (k < n) {
+        const float* src = Kd + (size_t)sE[k].x * ld + 32 * q;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          if (8 * q + t < ldc)
+            cp_async16(dst + 32 * t, src + 4 * t);
+          else
+            dst[32 * t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) dst[32 * t] = make_float4(1.f, 1.f, 1.f, 1.f);
+      }
     }
     // Next document's pointers (the order[] load has landed by now).
     int64_t bn = 0;
@@ -332,18 +355,12 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
     cp_async_wait_all();
     __syncwarp();
 
+    const uint2* const sEl = sE + rr * WPS + g;  // entries of staged round 0
     auto load_staged = [&](int s_round, Row& r, float& cval) {
-      const int s = s_round * WPS + g;
-      cval = __uint_as_float(sE[rr * WPS + s].y);
-#if WMD_SOLVE_PAD
-      const float4* rp = sK + (size_t)(s * LPW + q) * Sh::SLC;
+      cval = __uint_as_float(sEl[s_round * WPS].y);
+      const float4* rp = sKl + s_round * (WPS * Sh::NCH);
 #pragma unroll
-      for (int t = 0; t < 8; ++t) r.c[t] = rp[t];
-#else
-      const float4* rp = sK + (size_t)s * Sh::NCH + 8 * q;
-#pragma unroll
-      for (int t = 0; t < 8; ++t) r.c[t] = rp[t ^ key];
-#endif
+      for (int t = 0; t < 8; ++t) r.c[t] = rp[32 * t];
     };
     // A row from L2 (pad: the padding row for k >= n, else zeros).
     auto load_global = [&](const float* __restrict__ P, int k, Row& r,
@@ -377,7 +394,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
 #pragma unroll
       for (int w = NC / 2; w >= 1; w >>= 1)
 #pragma unroll
-        for (int i = 0; i < w; ++i) a[i] = make_float2(a[i].x + a[i + w].x, a[i].y + a[i + w].y);
+        for (int i = 0; i < w; ++i) a[i] = fadd2(a[i], a[i + w]);
       float s = a[0].x + a[0].y;
 #pragma unroll
       for (int off = 1; off < LPW; off <<= 1)
@@ -422,36 +439,33 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
       }
     };
     // Sum the x slices of all word slots: lane writes its 32 values as row
-    // `lane` of a 32x32 buffer (chunk-swizzled), then each lane sums, for
+    // `lane` of a 32x32 buffer (row pitch RP), then each lane sums, for
     // each of its LPW dimension groups, the slots' values of its dimension.
     // Paired form (LPW < 32): lanes L and L ^ 16 sum the dimension pair
     // (2p, 2p + 1), p = L % 16, over the two halves of the slots with 8-byte
     // loads and packed adds, combine the halves with one shuffle, and keep
     // dimension 2p + L / 16 (= own): tot[qq] is dimension 32*qq + own.
     auto reduce_slots = [&](const float2 (&x2)[16], float (&tot)[LPW]) {
-      float4* rw = reinterpret_cast<float4*>(red + lane * 32);
+      float4* rw = reinterpret_cast<float4*>(red + lane * Sh::RP);
 #pragma unroll
       for (int t = 0; t < 8; ++t)
-        rw[t ^ key] = make_float4(x2[2 * t].x, x2[2 * t].y, x2[2 * t + 1].x,
-                                  x2[2 * t + 1].y);
+        rw[t] = make_float4(x2[2 * t].x, x2[2 * t].y, x2[2 * t + 1].x, x2[2 * t + 1].y);
       __syncwarp();
       if constexpr (kPairSum) {
         constexpr int HALF = WPS / 2;
         const int p = lane & 15, h = lane >> 4;
+        const float* redp = red + h * HALF * LPW * Sh::RP + 2 * p;
 #pragma unroll
         for (int qq = 0; qq < LPW; ++qq) {
           float2 part[HALF];
 #pragma unroll
-          for (int i = 0; i < HALF; ++i) {
-            const int row = (h * HALF + i) * LPW + qq;
-            part[i] = *reinterpret_cast<const float2*>(
-                red + row * 32 + 4 * ((p >> 1) ^ (row & 7)) + 2 * (p & 1));
-          }
+          for (int i = 0; i < HALF; ++i)
+            part[i] = *reinterpret_cast<const float2*>(redp + (i * LPW + qq) * Sh::RP);
 #pragma unroll
           for (int w = HALF / 2; w >= 1; w >>= 1)
 #pragma unroll
             for (int i = 0; i < w; ++i)
-              part[i] = make_float2(part[i].x + part[i + w].x, part[i].y + part[i + w].y);
+              part[i] = fadd2(part[i], part[i + w]);
           const float2 o = make_float2(__shfl_xor_sync(0xffffffffu, part[0].x, 16),
                                        __shfl_xor_sync(0xffffffffu, part[0].y, 16));
           tot[qq] = h ? part[0].y + o.y : part[0].x + o.x;
@@ -461,10 +475,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
         for (int qq = 0; qq < LPW; ++qq) {
           float part[WPS];
 #pragma unroll
-          for (int gg = 0; gg < WPS; ++gg) {
-            const int row = gg * LPW + qq;
-            part[gg] = red[row * 32 + 4 * ((lane >> 2) ^ (row & 7)) + (lane & 3)];
-          }
+          for (int gg = 0; gg < WPS; ++gg) part[gg] = red[(gg * LPW + qq) * Sh::RP + lane];
 #pragma unroll
           for (int w = WPS / 2; w >= 1; w >>= 1)
 #pragma unroll
@@ -696,7 +707,7 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
                           const SourceSel& s, const Targets& t,
                           const SolveCtl& ctl, double* out, cudaStream_t st,
                           const GroupSrc* grp = nullptr, int nsrc = 0) {
-  using Sh = SolveShape<LPW>;
+  using Sh = SolveShape<LPW, RLX>;
   constexpr int kMaxDev = 64;
   constexpr int kBlocksPerSm = kC;
   constexpr int kWarps = kW;

@@ -115,6 +115,11 @@ int launch_gather_needed_f64(const double* src_mapped, uint64_t V, uint64_t d,
                              const uint2* ent, uint64_t nnz, const double* r_dev,
                              unsigned char* need, float* E32, float* nE,
                              unsigned long long* nrows, cudaStream_t st);
+// Rows narrowed to FP32 on the host: rows32 [count][d] in ascending word
+// order, slot[w] = row of word w in rows32 or -1 (row zeroed); E32 and nE
+// come out as launch_gather_needed_f64 writes them.
+int launch_scatter_rows(const float* rows32, const int32_t* slot, uint64_t V, uint64_t d,
+                        float* E32, float* nE, cudaStream_t st);
 
 // Targets: validated packing of a CSC triple into (col_ptr, ent).
 int launch_pack_targets(const uint64_t* col_ptr_in, const uint64_t* rows_in,
@@ -160,7 +165,10 @@ int launch_cdist_fp32(const float* E32, const float* nE, uint64_t V, uint64_t d,
 // form that reads E32/S directly (E16/S16 unused; needs d % 4 == 0).
 // Returns launches, or -1 if unsupported (tensor maps or shared-memory
 // budget).
-enum TcForm { TC_FP16 = 0, TC_BF16 = 1, TC_TF32X3 = 2 };
+// TC_F16X3: the split-FP16 form; E16 / S16 then hold split rows of
+// tc_split_row_bytes(d) bytes each (launch_to_split16): FP16 high part,
+// scaled FP16 low part, the row's 1/scale.
+enum TcForm { TC_FP16 = 0, TC_BF16 = 1, TC_TF32X3 = 2, TC_F16X3 = 3 };
 struct GroupSrc;
 // A stacked batch group's cost panel (batch.cu): N-tile y of the launch is
 // tiles[y] = {source, first stacked source row, first panel column, 0}, the
@@ -173,6 +181,10 @@ struct StackedPanels {
 int tc_padded_width(uint64_t d);
 int tc_tile_n(uint32_t cap, uint64_t d);
 int tc_tile_n_x3(uint32_t cap, uint64_t d);  // 0 = form unsupported
+int tc_tile_n_h2(uint32_t cap, uint64_t d);  // 0 = form unsupported
+size_t tc_split_row_bytes(uint64_t d);       // 4 * dp + 16
+int launch_to_split16(const float* E32, uint64_t rows, uint64_t d, void* Esplit,
+                      cudaStream_t st);
 int launch_to16(const float* E32, uint64_t rows, uint64_t d, void* E16,
                 bool bf16, cudaStream_t st);
 int launch_cdist_tc(int form, const void* E16, const void* S16,
