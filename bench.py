@@ -16,9 +16,10 @@ stream, L2 flushed between steps; the cost panel runs on tcgen05 from a
 resident split-FP16 copy of the embeddings, FP32-accurate and checked against
 the oracle at 1e-5 before timing; ``--cdist`` selects the other forms); ``e2e``
 is the same metric through the drop-in C ABI call with pinned host buffers
-(inside every step: H2D of r and the CSC matrix, the embedding rows of the
-words in the targets or the source narrowed FP64 -> FP32 by the host threads
-and copied while the next rows are converted, D2H of WMD;
+(inside every step: H2D of r and the CSC matrix; the embedding rows of a
+prefix of the vocabulary narrowed FP64 -> FP32 by the host threads and copied
+while the GPU reads the rows of the words in the targets or the source above
+it in FP64 from the pinned buffer; D2H of WMD;
 ``h2d_bytes_per_step`` counts what crossed the bus); ``roofline`` covers the
 dominant kernel; ``cpu_baseline`` times the reference's own OpenMP solver on
 this host.  ``--impl reference`` times only the reference's CPU solver.
@@ -950,18 +951,22 @@ def ours(a, rank, world, local):
     if world > 1:
         dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
         dist.all_reduce(res_tot, op=dist.ReduceOp.MAX)
-    # the same calls with the rows read in FP64 by the GPU from the pinned
-    # buffer (no host narrowing), for comparison
-    os.environ["WMD_DROPIN_NARROW"] = "0"
-    wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
-    h2d_dev = wmd.dropin_h2d_bytes()
-    dev_t = []
-    for _ in range(max(2, a.e2e_steps // 2)):
-        t0 = time.perf_counter()
+    # the same calls at other splits of the embedding rows between the host
+    # threads (a prefix of the vocabulary, narrowed to FP32) and the GPU's
+    # own FP64 reads of the needed rows above it from the pinned buffer
+    share_sweep = {}
+    for share in ("0", "0.1", "0.2", "0.3", "0.4", "0.5", "1"):
+        os.environ["WMD_DROPIN_HOST_SHARE"] = share
         wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
-        dev_t.append(time.perf_counter() - t0)
-    del os.environ["WMD_DROPIN_NARROW"]
-    dev_read_value = n_total * len(dev_t) / sum(dev_t)
+        sh_b = wmd.dropin_h2d_bytes()
+        sh_t = []
+        for _ in range(max(3, a.e2e_steps // 2)):
+            t0 = time.perf_counter()
+            wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
+            sh_t.append(time.perf_counter() - t0)
+        share_sweep[share] = {"pairs_per_s": n_total * len(sh_t) / sum(sh_t),
+                              "h2d_bytes_per_step": sh_b}
+    del os.environ["WMD_DROPIN_HOST_SHARE"]
     e2e_value = n_total * a.e2e_steps / float(e2e_tot.item())
     e2e_pcie_gbs = h2d * a.e2e_steps / float(e2e_tot.item()) / 1e9
     res_value = n_total * a.e2e_steps / float(res_tot.item())
@@ -1015,17 +1020,15 @@ def ours(a, rank, world, local):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "h2d_input_bytes": h2d_full,
                     "api": ("wmd_sinkhorn_fused_csc (drop-in, pinned host "
-                            "buffers: only the embedding rows of words in the "
-                            "targets or the source move, narrowed to FP32 by "
-                            f"the host threads ({host_cores()}) and copied in "
-                            "chunks overlapping the conversion; FP32-accurate "
-                            "split-TF32 tcgen05 cost panel)"),
+                            "buffers: the rows of a prefix of the vocabulary "
+                            "narrowed to FP32 by the host threads "
+                            f"({host_cores()}) and copied in chunks while the "
+                            "GPU reads the rows of the words in the targets or "
+                            "the source above it in FP64 from the pinned "
+                            "buffer; FP32-accurate split-TF32 tcgen05 cost "
+                            "panel)"),
                     "h2d_gbs": e2e_pcie_gbs,
-                    "device_read_value": dev_read_value,
-                    "device_read_h2d_bytes_per_step": h2d_dev,
-                    "device_read": ("the same call with WMD_DROPIN_NARROW=0: the "
-                                    "GPU reads the FP64 rows from the pinned "
-                                    "buffer itself"),
+                    "host_share_sweep": share_sweep,
                     "resident_corpus_value": res_value,
                     "resident_corpus_h2d_bytes_per_step": p.V * 8,
                     "max_rel_err_vs_oracle": e2e_err},

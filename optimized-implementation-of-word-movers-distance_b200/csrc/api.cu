@@ -159,14 +159,14 @@ struct wmd_handle {
   int64_t tc_long[4][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
   // embeddings
   DevBuf E32, nE, E64_stage, E16;
-  DevBuf need, need_count;  // needed-rows upload of the drop-in calls
-  // Drop-in rows narrowed to FP32 on the host: pinned staging [slot[V] |
-  // rows], their device copies, and the host marks / ids of needed words.
+  // Drop-in rows: flags of the needed words and the count of rows read over
+  // the bus; pinned staging of the host-narrowed prefix and its device copy.
+  DevBuf need, need_count;
   HostBuf hstage;
-  DevBuf rows32, slot_dev;
-  std::vector<unsigned char> hmark;
-  std::vector<uint32_t> hids;
+  DevBuf rows32;
   uint64_t dropin_h2d = 0;  // bytes the last drop-in call moved host -> device
+  // rows of the last drop-in call narrowed on the host / read by the GPU
+  uint64_t dropin_host_rows = 0, dropin_dev_rows = 0;
   uint64_t V = 0, d = 0;
   bool have_E = false;
   int e16_fmt = -1;  // format E16 holds (1 bf16, 2 fp16), -1 = stale
@@ -238,6 +238,7 @@ struct wmd_handle {
   // stage timing
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_split = nullptr;  // drop-in: host-row copies done (stream2)
   // CUDA-graph replay of device queries; graph_epoch changes whenever a
   // buffer or setting a captured graph depends on changes.
   bool use_graphs = true;
@@ -1546,30 +1547,76 @@ const void* mapped_host_range(const void* p, size_t bytes) {
   return a.devicePointer;
 }
 
-// Drop-in embeddings from device-mapped host memory: only the rows of the
-// words the query can touch (the targets already set, the source words of r)
-// cross the bus.  Leaves r uploaded in r_dev.  The handle's E then holds
-// zeros for every other word, so it is only valid for this target set and
-// this r — which is how the drop-in calls use their private handle.
-wmd_status set_embeddings_needed(wmd_handle* h, const double* vecs_mapped,
-                                 const double* r, uint64_t V, uint64_t d) {
+// Drop-in embeddings, split two ways so that the host threads and the host
+// bus work at the same time:
+//   * the rows of the words below wh = host_share * V (all of them when the
+//     embeddings are not device-mapped) are converted FP64 -> FP32 by the
+//     host threads into pinned memory, chunk by chunk, each chunk copied to
+//     the device on the second stream while the next one is converted (4
+//     bytes per entry on the bus; every word of the prefix, needed or not:
+//     the low ids are the frequent words, nearly all of them needed);
+//   * above wh the GPU flags the words a query can touch (the target words of
+//     the resident target set and the source words r != 0) and reads their
+//     rows in FP64 straight from the caller's device-mapped memory (8 bytes
+//     per entry), meanwhile; every other row is zeroed.
+// Both conversions round FP64 to FP32 to nearest and the norms are summed in
+// one order, so the results are bit-identical whatever the split.  The
+// handle's E then holds zeros for unneeded words above wh, so it is only
+// valid for this target set and this r, which is how the drop-in calls use
+// their private handle.  Leaves r uploaded in r_dev.
+wmd_status set_embeddings_split(wmd_handle* h, const double* vecs, const double* vmap,
+                                const double* r, uint64_t V, uint64_t d, double host_share,
+                                uint64_t* host_rows, uint64_t* dev_rows) {
   if (V > 0xFFFFFFFFull)
     return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^32 words");
   if (d > 65536) return fail(WMD_ERR_UNSUPPORTED, "embedding width above 65536");
   if (!h->have_T || h->tV != V)
     return fail(WMD_ERR_INVALID_ARG, "targets must be set first");
+  uint64_t wh = vmap ? (uint64_t)(host_share * (double)V + 0.5) : V;
+  if (wh > V) wh = V;
   const size_t n = (size_t)V * d;
   CK(h->E32.ensure(n * sizeof(float)));
   CK(h->nE.ensure((size_t)V * sizeof(float)));
-  CK(h->need.ensure((size_t)V));
-  CK(h->need_count.ensure(2 * sizeof(unsigned long long)));
   CK(h->r_dev.ensure(V * sizeof(double)));
-  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice,
-                     h->stream));
-  int launches = launch_gather_needed_f64(
-      vecs_mapped, V, d, h->ent.as<uint2>(), h->nnz, h->r_dev.as<double>(),
-      h->need.as<unsigned char>(), h->E32.as<float>(), h->nE.as<float>(),
-      h->need_count.as<unsigned long long>(), h->stream);
+  CK(h->need.ensure((size_t)V));
+  CK(h->need_count.ensure(sizeof(unsigned long long)));
+  CK(h->rows32.ensure(std::max<size_t>(wh, 1) * d * sizeof(float)));
+  if (wh > 0) {
+    CK(h->hstage.ensure(std::max<size_t>(wh, 1) * d * sizeof(float)));
+    if (!h->stream2) CK(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
+    if (!h->ev_split) CK(cudaEventCreateWithFlags(&h->ev_split, cudaEventDisableTiming));
+  }
+  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  // The GPU's share: starts now.
+  int launches = launch_gather_rows_split(vmap, h->ent.as<uint2>(), h->nnz,
+                                          h->r_dev.as<double>(), h->need.as<unsigned char>(),
+                                          V, d, wh, nullptr, 0, h->E32.as<float>(),
+                                          h->nE.as<float>(),
+                                          h->need_count.as<unsigned long long>(), h->stream);
+  // The host's share, in chunks of about 8 MB of FP32 (at least 8 chunks when
+  // there are enough rows), each copied on the second stream while the next
+  // one is converted.
+  if (wh > 0) {
+    float* rows = static_cast<float*>(h->hstage.p);
+    const uint64_t per_chunk =
+        std::max<uint64_t>(1, std::min<uint64_t>((8u << 20) / (d * 4) + 1, (wh + 7) / 8));
+    for (uint64_t i0 = 0; i0 < wh; i0 += per_chunk) {
+      const uint64_t i1 = std::min(wh, i0 + per_chunk);
+      const int64_t e0 = (int64_t)(i0 * d), e1 = (int64_t)(i1 * d);
+#pragma omp parallel for schedule(static)
+      for (int64_t e = e0; e < e1; ++e) rows[e] = (float)vecs[e];
+      CK(cudaMemcpyAsync(h->rows32.as<float>() + i0 * d, rows + i0 * d,
+                         (size_t)(i1 - i0) * d * sizeof(float), cudaMemcpyHostToDevice,
+                         h->stream2));
+    }
+    CK(cudaEventRecord(h->ev_split, h->stream2));
+    CK(cudaStreamWaitEvent(h->stream, h->ev_split, 0));
+    launches += launch_gather_rows_split(vmap, h->ent.as<uint2>(), h->nnz,
+                                         h->r_dev.as<double>(), h->need.as<unsigned char>(),
+                                         V, d, wh, h->rows32.as<float>(), 1,
+                                         h->E32.as<float>(), h->nE.as<float>(),
+                                         h->need_count.as<unsigned long long>(), h->stream);
+  }
   CK(cudaGetLastError());
   wmd_status se = update_emax(h, V);
   if (se) return se;
@@ -1584,92 +1631,15 @@ wmd_status set_embeddings_needed(wmd_handle* h, const double* vecs_mapped,
   for (int& x : h->warp_shape) x = -2;
   h->graph_epoch++;
   h->last_launches = launches;
+  *host_rows = wh;
+  *dev_rows = 0;  // known once the stream has run: dropin_csc reads need_count
   return WMD_OK;
 }
 
-// Drop-in embeddings narrowed on the host: the words a query can touch (the
-// target words of the resident target set, whose row indices the caller's
-// CSC holds and set_targets_csc has range-checked, and the source words
-// r != 0) are converted FP64 -> FP32 by the host threads into pinned memory,
-// chunk by chunk, each chunk copied to the device while the next one is
-// converted; a kernel then places the rows (and their norms) in E32 and
-// zeroes the rest.  The bus carries 4 bytes per needed entry instead of 8,
-// and the FP32 values are those the device-side conversion gives
-// (round to nearest), so the results are bit-identical to the other paths.
-wmd_status set_embeddings_host_rows(wmd_handle* h, const double* vecs, const double* r,
-                                    uint64_t V, uint64_t d, const uint64_t* row_inds,
-                                    uint64_t nnz, uint64_t* nrows) {
-  if (V > 0x7FFFFFFFull)
-    return fail(WMD_ERR_UNSUPPORTED, "vocabulary larger than 2^31-1 words");
-  if (d > 65536) return fail(WMD_ERR_UNSUPPORTED, "embedding width above 65536");
-  if (!h->have_T || h->tV != V)
-    return fail(WMD_ERR_INVALID_ARG, "targets must be set first");
-  // Needed words.
-  h->hmark.assign(V, 0);
-  unsigned char* mark = h->hmark.data();
-#pragma omp parallel for schedule(static)
-  for (int64_t e = 0; e < (int64_t)nnz; ++e)
-    __atomic_store_n(&mark[row_inds[e]], (unsigned char)1, __ATOMIC_RELAXED);
-  for (uint64_t w = 0; w < V; ++w)
-    if (r[w] != 0.0) mark[w] = 1;
-  // Pinned layout: slot[V] (int32, the row of each word in the row block or
-  // -1), then the row block at a 256-byte boundary.
-  const size_t slot_bytes = ((size_t)V * 4 + 255) & ~(size_t)255;
-  h->hids.clear();
-  for (uint64_t w = 0; w < V; ++w)
-    if (mark[w]) h->hids.push_back((uint32_t)w);
-  const uint64_t count = h->hids.size();
-  const size_t n = (size_t)V * d;
-  CK(h->E32.ensure(n * sizeof(float)));
-  CK(h->nE.ensure((size_t)V * sizeof(float)));
-  CK(h->r_dev.ensure(V * sizeof(double)));
-  CK(h->slot_dev.ensure((size_t)V * 4));
-  CK(h->rows32.ensure(std::max<size_t>(count, 1) * d * sizeof(float)));
-  CK(h->hstage.ensure(slot_bytes + std::max<size_t>(count, 1) * d * sizeof(float)));
-  int32_t* slot = static_cast<int32_t*>(h->hstage.p);
-  float* rows = reinterpret_cast<float*>(static_cast<char*>(h->hstage.p) + slot_bytes);
-  {
-    int32_t k = 0;
-    for (uint64_t w = 0; w < V; ++w) slot[w] = mark[w] ? k++ : -1;
-  }
-  CK(cudaMemcpyAsync(h->slot_dev.p, slot, (size_t)V * 4, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  // Rows, in chunks of about 8 MB of FP32 (at least 8 chunks when there are
-  // enough rows), so the copies overlap the conversion of later chunks.
-  const uint32_t* ids = h->hids.data();
-  const uint64_t per_chunk =
-      std::max<uint64_t>(1, std::min<uint64_t>((8u << 20) / (d * 4) + 1, (count + 7) / 8));
-  for (uint64_t i0 = 0; i0 < count; i0 += per_chunk) {
-    const uint64_t i1 = std::min(count, i0 + per_chunk);
-#pragma omp parallel for schedule(static)
-    for (int64_t i = (int64_t)i0; i < (int64_t)i1; ++i) {
-      const double* src = vecs + (uint64_t)ids[i] * d;
-      float* dst = rows + (uint64_t)i * d;
-      for (uint64_t k = 0; k < d; ++k) dst[k] = (float)src[k];
-    }
-    CK(cudaMemcpyAsync(h->rows32.as<float>() + i0 * d, rows + i0 * d,
-                       (size_t)(i1 - i0) * d * sizeof(float), cudaMemcpyHostToDevice,
-                       h->stream));
-  }
-  int launches = launch_scatter_rows(h->rows32.as<float>(), h->slot_dev.as<int32_t>(), V, d,
-                                     h->E32.as<float>(), h->nE.as<float>(), h->stream);
-  CK(cudaGetLastError());
-  wmd_status se = update_emax(h, V);
-  if (se) return se;
-  launches += 1;
-  h->V = V;
-  h->d = d;
-  h->have_E = true;
-  h->e16_fmt = -1;
-  h->ehl_ready = false;
-  h->ws_docs_ready = false;
-  for (int& x : h->blk_shape) x = -2;
-  for (int& x : h->warp_shape) x = -2;
-  h->graph_epoch++;
-  h->last_launches = launches;
-  *nrows = count;
-  return WMD_OK;
-}
+// Share of the vocabulary (a prefix of the word ids) whose rows the host
+// threads narrow in a drop-in call when the GPU can read the others itself
+// (measured on the B200 box's host, single-source workload).
+constexpr double kDropinHostShare = 0.5;
 
 // Per-host-thread default handle for the drop-in calls.
 struct TlHandle {
@@ -1721,29 +1691,28 @@ wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
   wmd_status s = default_handle(&h);
   if (s) return s;
   const uint64_t csc_bytes = (N + 1) * 8 + c->nnz * 16 + N * 4;  // + order
-  // Rows narrowed on the host when there are host threads to convert them
-  // (WMD_DROPIN_NARROW=0 turns this off): half the bus bytes of the FP64
-  // rows.  Otherwise pinned, device-mapped embeddings are read in place.
-  const char* nenv = getenv("WMD_DROPIN_NARROW");
-  const bool narrow = omp_get_max_threads() >= 4 && !(nenv && nenv[0] == '0');
-  const void* vmap =
-      narrow ? nullptr : mapped_host_range(vecs, (size_t)V * d * sizeof(double));
+  // Embedding rows.  With the embeddings in pinned, device-mapped memory the
+  // host threads narrow the rows of a prefix of the vocabulary to FP32 while
+  // the GPU reads the needed rows above it in FP64 (the prefix, as a share of
+  // V: WMD_DROPIN_HOST_SHARE in [0, 1], by default kDropinHostShare, none
+  // with fewer than 4 host threads); pageable embeddings are narrowed on the
+  // host whole, or copied whole when there are fewer than 4 host threads or
+  // the share is 0.
+  const double* vmap = static_cast<const double*>(
+      mapped_host_range(vecs, (size_t)V * d * sizeof(double)));
+  double share = omp_get_max_threads() >= 4 ? kDropinHostShare : 0.0;
+  if (const char* env = getenv("WMD_DROPIN_HOST_SHARE")) {
+    const double x = atof(env);
+    share = x < 0.0 ? 0.0 : x > 1.0 ? 1.0 : x;
+  }
+  const bool split = vmap || share > 0.0;
   int le = 0, lt = 0;
-  uint64_t nrows = 0;
-  if (narrow) {
+  uint64_t nh = 0, nd = 0;
+  if (split) {
     s = set_targets_csc(h, c);
     if (s) return s;
     lt = h->last_launches;
-    s = set_embeddings_host_rows(h, vecs, r, V, d, c->row_inds, c->nnz, &nrows);
-    if (s) return s;
-    le = h->last_launches;
-  } else if (vmap) {
-    // Pinned, device-mapped embeddings: targets first, then only the rows
-    // they (and the source) need are read over the bus.
-    s = set_targets_csc(h, c);
-    if (s) return s;
-    lt = h->last_launches;
-    s = set_embeddings_needed(h, static_cast<const double*>(vmap), r, V, d);
+    s = set_embeddings_split(h, vecs, vmap, r, V, d, share, &nh, &nd);
     if (s) return s;
     le = h->last_launches;
   } else {
@@ -1754,22 +1723,20 @@ wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
     if (s) return s;
     lt = h->last_launches;
   }
-  s = query_host(h, r, expo, max_iter, WMD, narrow || vmap != nullptr);
+  s = query_host(h, r, expo, max_iter, WMD, split);
   if (s) return s;
   h->last_launches += le + lt;
-  if (narrow) {  // CSC + r + the slot map + the FP32 rows
-    h->dropin_h2d = csc_bytes + V * 8 + V * 4 + nrows * d * 4;
-    return WMD_OK;
-  }
-  uint64_t rows = V;
-  if (vmap) {
+  if (split) {  // rows the GPU read over the bus (query_host synchronised)
     unsigned long long cnt = 0;
-    CK(cudaMemcpyAsync(&cnt, h->need_count.p, sizeof(cnt), cudaMemcpyDeviceToHost,
-                       h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    rows = cnt;
+    CK(cudaMemcpy(&cnt, h->need_count.p, sizeof(cnt), cudaMemcpyDeviceToHost));
+    nd = cnt;
   }
-  h->dropin_h2d = csc_bytes + V * 8 + rows * d * 8;
+  // bus bytes: CSC + r + the host-narrowed prefix (FP32) + the rows the GPU
+  // read (FP64), or the whole FP64 matrix
+  h->dropin_h2d = split ? csc_bytes + V * 8 + nh * d * 4 + nd * d * 8
+                        : csc_bytes + V * 8 + V * d * 8;
+  h->dropin_host_rows = nh;
+  h->dropin_dev_rows = nd;
   return WMD_OK;
 }
 
@@ -1866,6 +1833,7 @@ wmd_status wmd_destroy(wmd_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   for (int i = 0; i < 4; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->ev_split) cudaEventDestroy(h->ev_split);
   if (h->stream2) {
     cudaStreamSynchronize(h->stream2);
     cudaStreamDestroy(h->stream2);

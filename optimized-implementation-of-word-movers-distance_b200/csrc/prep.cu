@@ -92,13 +92,18 @@ int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
 }
 
 // ---------------------------------------------------------------------------
-// Needed rows only (drop-in calls whose FP64 embeddings sit in pinned,
-// device-mapped host memory): flag the words a query can touch — every target
-// word and every source word (r != 0) — then read exactly those rows over the
-// bus, convert them to FP32 with their norms, and zero the rest (a zero row
-// is finite and never near any source row, so the cost panel's unused rows
-// stay harmless; the solve never gathers them).
-// ---------------------------------------------------------------------------
+// Drop-in embedding rows split between the host and the bus (api.cu): the
+// rows of words below `wh` are narrowed FP64 -> FP32 by the host threads and
+// copied (rows32[w], every word of that id prefix); above it the GPU reads
+// the rows of the words a query can touch (flagged in `need`: every target
+// word and every source word) straight from the caller's device-mapped host
+// memory, and zeroes the others.  Phase 0 handles the words >= wh (it runs
+// while the host converts), phase 1 the prefix.  E32 and the norms come out
+// as embed_convert_f64_kernel and embed_norms_kernel write them for the whole
+// matrix (the same FP64 -> FP32 rounding, the same per-lane order of the FP64
+// norm sums), so the results do not depend on the split.  A zero row is
+// finite and never near any source row, so the cost panel's unused rows stay
+// harmless; the solve never gathers them.
 __global__ void mark_needed_kernel(const uint2* __restrict__ ent, uint64_t nnz,
                                    const double* __restrict__ r, uint64_t V,
                                    unsigned char* __restrict__ need) {
@@ -107,103 +112,80 @@ __global__ void mark_needed_kernel(const uint2* __restrict__ ent, uint64_t nnz,
   if (i < V && r[i] != 0.0) need[i] = 1;
 }
 
-__global__ void gather_convert_f64_kernel(const double* __restrict__ src, uint64_t V,
-                                          uint64_t d,
-                                          const unsigned char* __restrict__ need,
-                                          float* __restrict__ E32,
-                                          float* __restrict__ nE,
-                                          unsigned long long* __restrict__ nrows) {
+__global__ void gather_rows_split_kernel(const double* __restrict__ src_mapped,
+                                         const unsigned char* __restrict__ need,
+                                         uint64_t V, uint64_t d, uint64_t wh,
+                                         const float* __restrict__ rows32, int phase,
+                                         float* __restrict__ E32, float* __restrict__ nE,
+                                         unsigned long long* __restrict__ nrows) {
   const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= V) return;
+  if ((phase == 0) == (row < wh)) return;  // the other phase's row
   float* o = E32 + row * d;
-  if (!need[row]) {
-    for (uint64_t k = lane; k < d; k += 32) o[k] = 0.f;
-    if (lane == 0) nE[row] = 0.f;
-    return;
-  }
-  if (lane == 0) atomicAdd(nrows, 1ull);  // rows read over the bus
-  const double* s = src + row * d;
   double acc = 0.0;
-  if (d <= 512) {
-    // All of a lane's loads before any use: one bus round trip per row.
-    double v[16];
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const uint64_t k = (uint64_t)lane + 32u * t;
-      v[t] = k < d ? s[k] : 0.0;
-    }
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const uint64_t k = (uint64_t)lane + 32u * t;
-      const float f = (float)v[t];
-      if (k < d) o[k] = f;
-      acc += (double)f * (double)f;
-    }
-  } else {
+  if (row < wh) {
+    const float* s = rows32 + row * d;
     for (uint64_t k = lane; k < d; k += 32) {
-      const float f = (float)s[k];
+      const float f = s[k];
       o[k] = f;
       acc += (double)f * (double)f;
     }
-  }
-#pragma unroll
-  for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-  if (lane == 0) nE[row] = (float)acc;
-}
-
-int launch_gather_needed_f64(const double* src_mapped, uint64_t V, uint64_t d,
-                             const uint2* ent, uint64_t nnz, const double* r_dev,
-                             unsigned char* need, float* E32, float* nE,
-                             unsigned long long* nrows, cudaStream_t st) {
-  const int threads = 256;
-  cudaMemsetAsync(need, 0, V, st);
-  cudaMemsetAsync(nrows, 0, sizeof(unsigned long long), st);
-  const uint64_t n = nnz > V ? nnz : V;
-  mark_needed_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(
-      ent, nnz, r_dev, V, need);
-  gather_convert_f64_kernel<<<(unsigned)((V * 32 + threads - 1) / threads), threads, 0,
-                              st>>>(src_mapped, V, d, need, E32, nE, nrows);
-  return 2;
-}
-
-// Needed rows narrowed to FP32 on the host (drop-in calls, staged through
-// pinned memory by api.cu): rows32 holds the needed rows in ascending word order,
-// slot[w] the row of word w in rows32 or -1.  Writes E32 and the norms
-// exactly as gather_convert_f64_kernel does (the same per-lane order of the
-// FP64 norm sums), zeroes the rows nobody needs.
-__global__ void scatter_rows_kernel(const float* __restrict__ rows32,
-                                    const int32_t* __restrict__ slot, uint64_t V,
-                                    uint64_t d, float* __restrict__ E32,
-                                    float* __restrict__ nE) {
-  const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (row >= V) return;
-  float* o = E32 + row * d;
-  const int32_t sl = slot[row];
-  if (sl < 0) {
+  } else if (!need[row]) {
     for (uint64_t k = lane; k < d; k += 32) o[k] = 0.f;
     if (lane == 0) nE[row] = 0.f;
     return;
-  }
-  const float* s = rows32 + (uint64_t)sl * d;
-  double acc = 0.0;
-  for (uint64_t k = lane; k < d; k += 32) {
-    const float f = s[k];
-    o[k] = f;
-    acc += (double)f * (double)f;
+  } else {
+    if (lane == 0) atomicAdd(nrows, 1ull);  // rows read over the bus
+    const double* s = src_mapped + row * d;
+    if (d <= 512) {
+      // All of a lane's loads before any use: one bus round trip per row.
+      double v[16];
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        const uint64_t k = (uint64_t)lane + 32u * t;
+        v[t] = k < d ? s[k] : 0.0;
+      }
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        const uint64_t k = (uint64_t)lane + 32u * t;
+        const float f = (float)v[t];
+        if (k < d) o[k] = f;
+        acc += (double)f * (double)f;
+      }
+    } else {
+      for (uint64_t k = lane; k < d; k += 32) {
+        const float f = (float)s[k];
+        o[k] = f;
+        acc += (double)f * (double)f;
+      }
+    }
   }
 #pragma unroll
   for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if (lane == 0) nE[row] = (float)acc;
 }
 
-int launch_scatter_rows(const float* rows32, const int32_t* slot, uint64_t V, uint64_t d,
-                        float* E32, float* nE, cudaStream_t st) {
+int launch_gather_rows_split(const double* src_mapped, const uint2* ent, uint64_t nnz,
+                             const double* r_dev, unsigned char* need, uint64_t V,
+                             uint64_t d, uint64_t wh, const float* rows32, int phase,
+                             float* E32, float* nE, unsigned long long* nrows,
+                             cudaStream_t st) {
   const int threads = 256;
-  scatter_rows_kernel<<<(unsigned)((V * 32 + threads - 1) / threads), threads, 0, st>>>(
-      rows32, slot, V, d, E32, nE);
-  return 1;
+  int n = 0;
+  if (phase == 0) {
+    cudaMemsetAsync(nrows, 0, sizeof(unsigned long long), st);
+    if (wh < V) {
+      cudaMemsetAsync(need, 0, V, st);
+      const uint64_t m = nnz > V ? nnz : V;
+      mark_needed_kernel<<<(unsigned)((m + threads - 1) / threads), threads, 0, st>>>(
+          ent, nnz, r_dev, V, need);
+      ++n;
+    }
+  }
+  gather_rows_split_kernel<<<(unsigned)((V * 32 + threads - 1) / threads), threads, 0, st>>>(
+      src_mapped, need, V, d, wh, rows32, phase, E32, nE, nrows);
+  return n + 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -297,6 +279,52 @@ __device__ __forceinline__ void copy_row16(const unsigned short* __restrict__ sr
     for (int k = lane; k < dp / 8; k += 32) d4[k] = __ldg(s4 + k);
   } else {
     for (int k = lane; k < dp; k += 32) dst[k] = src[k];
+  }
+}
+
+__device__ __forceinline__ void copy_row(const float* __restrict__ src,
+                                         float* __restrict__ dst, uint64_t d,
+                                         int lane);
+
+// One source row for the cost panel, one warp: the FP32 row (d floats) and,
+// when s16 is given, its 16-bit (or split) row of dp values, with every load
+// issued before the first store (one memory round trip for both).
+__device__ __forceinline__ void gather_source_row(const float* __restrict__ src,
+                                                  float* __restrict__ dst, uint64_t d,
+                                                  const unsigned short* __restrict__ s16,
+                                                  unsigned short* __restrict__ d16, int dp,
+                                                  int lane) {
+  if (d <= 512 && (!s16 || (dp % 8 == 0 && dp <= 1024))) {
+    float v[16];
+    uint4 h[4];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t k = (uint64_t)lane + 32u * t;
+      v[t] = k < d ? __ldg(src + k) : 0.f;
+    }
+    if (s16) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int k = lane + 32 * t;
+        h[t] = k < dp / 8 ? __ldg(reinterpret_cast<const uint4*>(s16) + k)
+                          : make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t k = (uint64_t)lane + 32u * t;
+      if (k < d) dst[k] = v[t];
+    }
+    if (s16) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int k = lane + 32 * t;
+        if (k < dp / 8) reinterpret_cast<uint4*>(d16)[k] = h[t];
+      }
+    }
+  } else {
+    copy_row(src, dst, d, lane);
+    if (s16) copy_row16(s16, d16, dp, lane);
   }
 }
 
@@ -418,12 +446,11 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     const uint32_t pos = list_pos[s];
     if (pos >= cap) continue;
     const uint64_t id = list_id[s];
-    const float* src = E32 + id * d;
-    float* dst = S + (uint64_t)pos * d;
-    copy_row(src, dst, d, lane);
     if (lane == 0) nS[pos] = nE[id];
-    if (S16)  // 16-bit (or split) row for the tensor-core cost panel
-      copy_row16(E16 + id * (uint64_t)dp, S16 + (uint64_t)pos * dp, dp, lane);
+    // FP32 row and, for the tensor-core cost panel, its 16-bit (or split) row
+    gather_source_row(E32 + id * d, S + (uint64_t)pos * d, d,
+                      S16 ? E16 + id * (uint64_t)dp : nullptr,
+                      S16 ? S16 + (uint64_t)pos * dp : nullptr, dp, lane);
   }
 }
 
@@ -465,11 +492,10 @@ __global__ void gather_sources_kernel(const uint32_t* __restrict__ ids, int coun
   const int lane = threadIdx.x & 31;
   if (w >= count) return;
   const uint64_t id = ids[w];
-  const float* src = E32 + id * d;
-  float* dst = S + (uint64_t)w * d;
-  copy_row(src, dst, d, lane);
   if (lane == 0) nS[w] = nE[id];
-  if (S16) copy_row16(E16 + id * (uint64_t)dp, S16 + (uint64_t)w * dp, dp, lane);
+  gather_source_row(E32 + id * d, S + (uint64_t)w * d, d,
+                    S16 ? E16 + id * (uint64_t)dp : nullptr,
+                    S16 ? S16 + (uint64_t)w * dp : nullptr, dp, lane);
 }
 
 int launch_gather_sources(const uint32_t* ids, int count, const float* E32,

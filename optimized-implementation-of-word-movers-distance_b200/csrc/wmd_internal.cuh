@@ -107,19 +107,17 @@ int launch_embed_norms(const float* E32, uint64_t V, uint64_t d, float* nE,
 // BF16 embeddings [V][d] (raw bit patterns) -> E32 (exact) and E16 [V][dp].
 int launch_embed_from_bf16(const void* src, uint64_t V, uint64_t d, int dp, float* E32,
                            void* E16, cudaStream_t st);
-// Rows of the words a query can touch (target words in `ent`, source words
-// r_dev != 0) read from device-mapped host memory and converted; all other
-// rows zeroed.  `need` is V bytes of scratch; *nrows receives the number of
-// rows read.
-int launch_gather_needed_f64(const double* src_mapped, uint64_t V, uint64_t d,
-                             const uint2* ent, uint64_t nnz, const double* r_dev,
-                             unsigned char* need, float* E32, float* nE,
-                             unsigned long long* nrows, cudaStream_t st);
-// Rows narrowed to FP32 on the host: rows32 [count][d] in ascending word
-// order, slot[w] = row of word w in rows32 or -1 (row zeroed); E32 and nE
-// come out as launch_gather_needed_f64 writes them.
-int launch_scatter_rows(const float* rows32, const int32_t* slot, uint64_t V, uint64_t d,
-                        float* E32, float* nE, cudaStream_t st);
+// Drop-in rows split between the host and the bus: words below wh from
+// rows32 (narrowed on the host; phase 1), above it the rows of the words a
+// query can touch (target words in `ent`, source words r_dev != 0; flags in
+// `need`, V bytes of scratch) read from device-mapped host memory, the others
+// zeroed (phase 0; *nrows receives the rows read over the bus).  E32 and nE
+// come out as launch_embed_convert_f64 writes them for the whole matrix.
+int launch_gather_rows_split(const double* src_mapped, const uint2* ent, uint64_t nnz,
+                             const double* r_dev, unsigned char* need, uint64_t V,
+                             uint64_t d, uint64_t wh, const float* rows32, int phase,
+                             float* E32, float* nE, unsigned long long* nrows,
+                             cudaStream_t st);
 
 // Targets: validated packing of a CSC triple into (col_ptr, ent).
 int launch_pack_targets(const uint64_t* col_ptr_in, const uint64_t* rows_in,
