@@ -955,7 +955,7 @@ def ours(a, rank, world, local):
     # threads (a prefix of the vocabulary, narrowed to FP32) and the GPU's
     # own FP64 reads of the needed rows above it from the pinned buffer
     share_sweep = {}
-    for share in ("0", "0.1", "0.2", "0.3", "0.4", "0.5", "1"):
+    for share in ("0", "0.3", "0.4", "0.5", "0.6", "0.7", "0.8", "1"):
         os.environ["WMD_DROPIN_HOST_SHARE"] = share
         wmd.sinkhorn_wmd_csc(*args, -p.lam, p.max_iter, "fused")
         sh_b = wmd.dropin_h2d_bytes()

@@ -164,6 +164,7 @@ struct wmd_handle {
   DevBuf need, need_count;
   HostBuf hstage;
   DevBuf rows32;
+  std::vector<int32_t> ord_host;  // document order of the last target set
   uint64_t dropin_h2d = 0;  // bytes the last drop-in call moved host -> device
   // rows of the last drop-in call narrowed on the host / read by the GPU
   uint64_t dropin_host_rows = 0, dropin_dev_rows = 0;
@@ -366,7 +367,12 @@ void length_order(const uint64_t* col_ptr, uint64_t N, std::vector<int32_t>& ord
   for (uint64_t j = 0; j < N; ++j) ord[cnt[bucket(j)]++] = (int32_t)j;
 }
 
-wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
+// defer_check: return once the copies and the packing are enqueued; the
+// caller synchronises later with finish(h) (which reports invalid indices or
+// values) and may only enqueue work that tolerates unchecked word ids until
+// then.
+wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c,
+                           bool defer_check = false) {
   if (!h || !c) return fail(WMD_ERR_INVALID_ARG, "set_targets: null argument");
   const uint64_t V = c->num_rows, N = c->num_cols, nnz = c->nnz;
   if (V == 0 || N == 0)
@@ -384,7 +390,7 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
       return fail(WMD_ERR_INVALID_INPUT, "column pointers decrease");
   wmd_status s = bind(h);
   if (s) return s;
-  std::vector<int32_t> ord;
+  std::vector<int32_t>& ord = h->ord_host;  // outlives its async copy
   length_order(c->col_ptr, N, ord);
   CK(h->stage_cp.ensure((N + 1) * sizeof(uint64_t)));
   CK(h->stage_rows.ensure(nnz * sizeof(uint64_t)));
@@ -408,8 +414,10 @@ wmd_status set_targets_csc(wmd_handle* h, const wmd_csc_double_t* c) {
       h->ent.as<uint2>(), h->err_dev.as<unsigned>(), h->stream);
   CK(cudaGetLastError());
   h->have_T = false;
-  s = finish(h);  // the order vector must outlive its async copy
-  if (s) return s;
+  if (!defer_check) {
+    s = finish(h);
+    if (s) return s;
+  }
   h->tV = V;
   h->N = N;
   h->nnz = nnz;
@@ -1709,12 +1717,19 @@ wmd_status dropin_csc(const double* r, const double* vecs, double* WMD,
   int le = 0, lt = 0;
   uint64_t nh = 0, nd = 0;
   if (split) {
-    s = set_targets_csc(h, c);
+    // The targets' copies and packing, the GPU's row reads and the host's
+    // conversion all overlap; the targets' checks are read afterwards.
+    s = set_targets_csc(h, c, true);
     if (s) return s;
     lt = h->last_launches;
     s = set_embeddings_split(h, vecs, vmap, r, V, d, share, &nh, &nd);
     if (s) return s;
     le = h->last_launches;
+    s = finish(h);
+    if (s) {
+      h->have_T = false;
+      return s;
+    }
   } else {
     s = set_embeddings(h, vecs, V, d, 0, true);
     if (s) return s;

@@ -194,23 +194,12 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
   float* ss_s = nS_s + p.NT;  // H2: source row scales
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  grid_dep_launch();
   // This CTA's N-tile: its first stacked source row (TMA, norms, near-pair
   // ids), its first panel column, and the panel it writes.
-  int n0 = blockIdx.y * p.NT, col0 = n0, vr, ldk = p.ld;
+  int n0 = blockIdx.y * p.NT, col0 = n0, vr = 0, ldk = p.ld;
   float* Kt = p.K;
   float* mrowt = p.mrow;
-  if (p.tiles) {
-    const int4 tl = p.tiles[blockIdx.y];
-    const GroupSrc& gs = p.grp[tl.x];
-    n0 = tl.y;
-    col0 = tl.z;
-    vr = gs.vr;
-    ldk = gs.ld;
-    Kt = gs.K;
-    mrowt = gs.mrow;
-  } else {
-    vr = (int)*p.vr;
-  }
   const int ntiles = (int)((p.V + BM - 1) / BM);
 
   if (threadIdx.x == 0) {
@@ -236,6 +225,21 @@ cdist_tc_kernel(const __grid_constant__ CUtensorMap tmA,
             smem_u32(tmem_slot)),
         "r"((uint32_t)p.tmem_cols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // Everything above touches only this CTA's shared and tensor memory; the
+  // source rows, their norms and v_r come from the selection before it.
+  grid_dep_wait();
+  if (p.tiles) {
+    const int4 tl = p.tiles[blockIdx.y];
+    const GroupSrc& gs = p.grp[tl.x];
+    n0 = tl.y;
+    col0 = tl.z;
+    vr = gs.vr;
+    ldk = gs.ld;
+    Kt = gs.K;
+    mrowt = gs.mrow;
+  } else {
+    vr = (int)*p.vr;
   }
   for (int c = threadIdx.x; c < p.NT; c += blockDim.x) {
     nS_s[c] = col0 + c < vr ? p.nS[n0 + c] : 0.f;
@@ -787,22 +791,22 @@ int launch_cdist_tc(int form, const void* E16, const void* S16,
     set_smem_attr<true>();
     const uint32_t idesc = tc::make_idesc(2, BM_ROWS, NT);
     const uint32_t idesc2 = tc::make_idesc(2, BM_ROWS, 2 * NT);
-    tc::cdist_tc_kernel<true><<<grid, tc::Form<true>::kThreads,
-                                tc::smem_bytes<true>(NT, KT, p.stages), st>>>(
-        tmA, tmB, tmA2, tmB2, p, idesc, idesc2);
+    launch_pdl(tc::cdist_tc_kernel<true>, grid, dim3(tc::Form<true>::kThreads),
+               tc::smem_bytes<true>(NT, KT, p.stages), st, tmA, tmB, tmA2, tmB2, p, idesc,
+               idesc2);
   } else if (h2) {
     set_smem_attr<false, true>();
     const uint32_t idesc = tc::make_idesc(0, BM_ROWS, NT);
     const uint32_t idesc2 = tc::make_idesc(0, BM_ROWS, 2 * NT);
-    tc::cdist_tc_kernel<false, true><<<grid, tc::Form<false, true>::kThreads,
-                                       tc::smem_bytes<false, true>(NT, KT, p.stages), st>>>(
-        tmA, tmB, tmA2, tmB2, p, idesc, idesc2);
+    launch_pdl(tc::cdist_tc_kernel<false, true>, grid, dim3(tc::Form<false, true>::kThreads),
+               tc::smem_bytes<false, true>(NT, KT, p.stages), st, tmA, tmB, tmA2, tmB2, p,
+               idesc, idesc2);
   } else {
     set_smem_attr<false>();
     const uint32_t idesc = tc::make_idesc(form == TC_BF16 ? 1 : 0, BM_ROWS, NT);
-    tc::cdist_tc_kernel<false><<<grid, tc::Form<false>::kThreads,
-                                 tc::smem_bytes<false>(NT, KT, p.stages), st>>>(
-        tmA, tmB, tmA2, tmB2, p, idesc, idesc);
+    launch_pdl(tc::cdist_tc_kernel<false>, grid, dim3(tc::Form<false>::kThreads),
+               tc::smem_bytes<false>(NT, KT, p.stages), st, tmA, tmB, tmA2, tmB2, p, idesc,
+               idesc);
   }
   return 1;
 }

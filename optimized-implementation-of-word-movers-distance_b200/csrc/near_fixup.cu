@@ -28,6 +28,8 @@ __global__ void near_fixup_kernel(NearList nl, float expo, float* __restrict__ K
   const int lane = threadIdx.x & 31;
   const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  grid_dep_launch();
+  grid_dep_wait();  // the cost panel's list and panel
   const unsigned total = *nl.count;
   const unsigned listed = total < nl.cap ? total : nl.cap;
   auto fix = [&](uint64_t w, int i) {
@@ -75,8 +77,8 @@ int launch_near_fixup(const NearList& near, float expo, float* K, float* KM,
                       int ld, uint64_t V, const float* nE, const float* nS,
                       const uint32_t* vr, int num_sms, cudaStream_t st, bool scaled) {
   const int threads = 256;
-  near_fixup_kernel<<<num_sms > 0 ? num_sms : 148, threads, 0, st>>>(
-      near, expo, K, KM, ld, V, nE, nS, vr, scaled);
+  launch_pdl(near_fixup_kernel, dim3(num_sms > 0 ? num_sms : 148), dim3(threads), 0, st,
+             near, expo, K, KM, ld, V, nE, nS, vr, scaled);
   return 1;
 }
 

@@ -108,7 +108,8 @@ __global__ void mark_needed_kernel(const uint2* __restrict__ ent, uint64_t nnz,
                                    const double* __restrict__ r, uint64_t V,
                                    unsigned char* __restrict__ need) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nnz) need[ent[i].x] = 1;  // ids were range-checked when packed
+  // (the packing's range check may not have been read yet: skip bad ids)
+  if (i < nnz && ent[i].x < V) need[ent[i].x] = 1;
   if (i < V && r[i] != 0.0) need[i] = 1;
 }
 
@@ -353,6 +354,7 @@ select_count_kernel(const double* __restrict__ r, uint64_t V,
                     uint32_t* __restrict__ chunk_counts,
                     unsigned* __restrict__ err, unsigned* __restrict__ zero_word) {
   __shared__ unsigned red[33];
+  grid_dep_launch();
   // A counter of a later kernel of the same query (the near-pair list), reset
   // here instead of by a separate memset on the stream.
   if (zero_word && blockIdx.x == 0 && threadIdx.x == 0) *zero_word = 0u;
@@ -388,6 +390,7 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
   __shared__ unsigned warp_off[kSelectThreads / 32];
   __shared__ uint32_t list_pos[kSelectChunk];
   __shared__ uint32_t list_id[kSelectChunk];
+  grid_dep_launch();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t base = (uint64_t)blockIdx.x * kSelectChunk;
   // This chunk's weights first: their loads overlap the offset computation.
@@ -398,7 +401,9 @@ select_write_kernel(const double* __restrict__ r, uint64_t V,
     rv[k] = i < V ? r[i] : 0.0;
   }
 
-  // Offset of this chunk = selected count of all chunks before it.
+  // Offset of this chunk = selected count of all chunks before it (the
+  // count kernel's output).
+  grid_dep_wait();
   unsigned before = 0, all = 0;
   for (int c = threadIdx.x; c < nchunks; c += blockDim.x) {
     const unsigned v = chunk_counts[c];
@@ -468,10 +473,10 @@ int launch_select(const double* r, uint64_t V, const float* E32,
   const int nchunks = select_num_chunks(V);
   select_count_kernel<<<nchunks, kSelectThreads, 0, st>>>(r, V, s.chunk_counts, err,
                                                           zero_word);
-  select_write_kernel<<<nchunks, kSelectThreads, 0, st>>>(
-      r, V, E32, nE, d, nchunks, s.chunk_counts, s.cap, s.ids, s.rinv, s.S,
-      s.nS, s.vr, err, static_cast<const unsigned short*>(E16),
-      static_cast<unsigned short*>(S16), dp);
+  launch_pdl(select_write_kernel, dim3(nchunks), dim3(kSelectThreads), 0, st, r, V, E32, nE,
+             d, nchunks, (const uint32_t*)s.chunk_counts, s.cap, s.ids, s.rinv, s.S, s.nS,
+             s.vr, err, static_cast<const unsigned short*>(E16),
+             static_cast<unsigned short*>(S16), dp);
   return 2;
 }
 

@@ -198,6 +198,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
   // the whole document loop (which spilled the wide instantiations).
   __shared__ __align__(16) unsigned char gs_raw[GRP ? kW * sizeof(GroupSrc) : 16];
   GroupSrc& gs = reinterpret_cast<GroupSrc*>(gs_raw)[GRP ? warp : 0];
+  grid_dep_wait();  // the panel (cost panel, fix-up) and the selection
   const int vr_arg = GRP ? 0 : (int)*vr_dev;
   auto KP = [&]() -> const float* {
     if constexpr (GRP) return gs.K;
@@ -738,10 +739,10 @@ static int launch_solve_t(const float* K, const float* KM, int ld, float expo,
   int64_t grid = (int64_t)sms_cache[dev] * kBlocksPerSm;
   if (grid > want) grid = want;
   if (grid < 1) grid = 1;
-  solve_kernel<LPW, FROM_KM, RLX, GRP, kW, kC><<<(unsigned)grid, kWarps * 32, smem, st>>>(
-      K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent, t.order, t.N,
-      ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega, ctl.vstate,
-      ctl.mrow, out, grp, nsrc);
+  launch_pdl(solve_kernel<LPW, FROM_KM, RLX, GRP, kW, kC>, dim3((unsigned)grid),
+             dim3(kWarps * 32), smem, st, K, KM, ld, expo, s.vr, s.rinv, t.col_ptr, t.ent,
+             t.order, t.N, ctl.max_iter, ctl.tol, ctl.iters, sr, ctl.u0, ctl.ldu, ctl.omega,
+             ctl.vstate, ctl.mrow, out, grp, nsrc);
   return 1;
 }
 
