@@ -240,6 +240,7 @@ struct wmd_handle {
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_split = nullptr;  // drop-in: host-row copies done (stream2)
+  cudaEvent_t ev_slot[4] = {nullptr, nullptr, nullptr, nullptr};  // staging slots free
   // CUDA-graph replay of device queries; graph_epoch changes whenever a
   // buffer or setting a captured graph depends on changes.
   bool use_graphs = true;
@@ -1555,6 +1556,14 @@ const void* mapped_host_range(const void* p, size_t bytes) {
   return a.devicePointer;
 }
 
+// Pinned staging of the drop-in calls' host-narrowed rows: a ring of slots
+// of about 8 MB (at least one row of d floats each).
+constexpr int kStageSlots = 4;
+inline size_t kStageSlotBytes(uint64_t d) {
+  const size_t row = (size_t)d * sizeof(float);
+  return std::max<size_t>(row, ((size_t)8 << 20) / row * row);
+}
+
 // Drop-in embeddings, split two ways so that the host threads and the host
 // bus work at the same time:
 //   * the rows of the words below wh = host_share * V (all of them when the
@@ -1590,9 +1599,11 @@ wmd_status set_embeddings_split(wmd_handle* h, const double* vecs, const double*
   CK(h->need_count.ensure(sizeof(unsigned long long)));
   CK(h->rows32.ensure(std::max<size_t>(wh, 1) * d * sizeof(float)));
   if (wh > 0) {
-    CK(h->hstage.ensure(std::max<size_t>(wh, 1) * d * sizeof(float)));
+    CK(h->hstage.ensure(kStageSlots * kStageSlotBytes(d)));
     if (!h->stream2) CK(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
     if (!h->ev_split) CK(cudaEventCreateWithFlags(&h->ev_split, cudaEventDisableTiming));
+    for (cudaEvent_t& e : h->ev_slot)
+      if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   CK(cudaMemcpyAsync(h->r_dev.p, r, V * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   // The GPU's share: starts now.
@@ -1603,19 +1614,26 @@ wmd_status set_embeddings_split(wmd_handle* h, const double* vecs, const double*
                                           h->need_count.as<unsigned long long>(), h->stream);
   // The host's share, in chunks of about 8 MB of FP32 (at least 8 chunks when
   // there are enough rows), each copied on the second stream while the next
-  // one is converted.
+  // one is converted; the chunks go through a ring of kStageSlots pinned
+  // slots, a slot reused once its copy is done, so the pinned memory stays
+  // kStageSlots x 8 MB whatever the vocabulary.
   if (wh > 0) {
-    float* rows = static_cast<float*>(h->hstage.p);
-    const uint64_t per_chunk =
-        std::max<uint64_t>(1, std::min<uint64_t>((8u << 20) / (d * 4) + 1, (wh + 7) / 8));
-    for (uint64_t i0 = 0; i0 < wh; i0 += per_chunk) {
+    const uint64_t per_chunk = std::max<uint64_t>(
+        1, std::min<uint64_t>(kStageSlotBytes(d) / (d * 4), (wh + 7) / 8));
+    uint64_t k = 0;
+    for (uint64_t i0 = 0; i0 < wh; i0 += per_chunk, ++k) {
       const uint64_t i1 = std::min(wh, i0 + per_chunk);
-      const int64_t e0 = (int64_t)(i0 * d), e1 = (int64_t)(i1 * d);
+      const int slot = (int)(k % kStageSlots);
+      if (k >= (uint64_t)kStageSlots) CK(cudaEventSynchronize(h->ev_slot[slot]));
+      float* rows = reinterpret_cast<float*>(static_cast<char*>(h->hstage.p) +
+                                             (size_t)slot * kStageSlotBytes(d));
+      const double* src = vecs + i0 * d;
+      const int64_t n = (int64_t)((i1 - i0) * d);
 #pragma omp parallel for schedule(static)
-      for (int64_t e = e0; e < e1; ++e) rows[e] = (float)vecs[e];
-      CK(cudaMemcpyAsync(h->rows32.as<float>() + i0 * d, rows + i0 * d,
-                         (size_t)(i1 - i0) * d * sizeof(float), cudaMemcpyHostToDevice,
-                         h->stream2));
+      for (int64_t e = 0; e < n; ++e) rows[e] = (float)src[e];
+      CK(cudaMemcpyAsync(h->rows32.as<float>() + i0 * d, rows, (size_t)n * sizeof(float),
+                         cudaMemcpyHostToDevice, h->stream2));
+      CK(cudaEventRecord(h->ev_slot[slot], h->stream2));
     }
     CK(cudaEventRecord(h->ev_split, h->stream2));
     CK(cudaStreamWaitEvent(h->stream, h->ev_split, 0));
@@ -1849,6 +1867,8 @@ wmd_status wmd_destroy(wmd_handle* h) {
   for (int i = 0; i < 4; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->ev_split) cudaEventDestroy(h->ev_split);
+  for (cudaEvent_t e : h->ev_slot)
+    if (e) cudaEventDestroy(e);
   if (h->stream2) {
     cudaStreamSynchronize(h->stream2);
     cudaStreamDestroy(h->stream2);
