@@ -58,9 +58,10 @@ def test_large_lambda_m_vs_oracle(wmd, synth, oracle_mod, alpha, v_r, prec):
     assert err.max() <= tol, f"max rel err {err.max():.3e}"
 
 
-@pytest.mark.parametrize("mode", ["fp32", "tf32x3", "bf16"])
+@pytest.mark.parametrize("mode", ["fp32", "tf32x3", "f16x3", "bf16"])
 def test_large_lambda_m_cost_panels_and_batch(wmd, synth, oracle_mod, mode):
-    """Every cost-panel form and the batched path take the row-scaled form."""
+    """Every cost-panel form and the batched path take the row-scaled form
+    (the split-FP16 form for the single query; its batches run split-TF32)."""
     p = _case(synth, 6.0, 40, 91)
     srcs = [p.r] + [synth.source_doc(p.V, v, seed=400 + v) for v in (12, 90)]
     refs = [oracle_mod.sinkhorn(r, p.vecs.astype(np.float64), p.col_ptr, p.row_inds,
