@@ -116,10 +116,14 @@ wmd_status wmd_sinkhorn_nonfused_csc(const double* r, const double* vecs,
 /* Host -> device bytes moved by the calling thread's last successful drop-in
  * call above (target matrix, r, embedding rows).  When `vecs` lies in one
  * pinned, device-mapped host allocation (cudaHostAlloc / cudaMallocHost /
- * cudaHostRegister), the GPU reads only the rows of the words that occur in
- * the target matrix or in r, directly from host memory; otherwise the whole
- * V x d matrix is copied.  Results are the same either way.  No reference
- * counterpart (a measurement aid). */
+ * cudaHostRegister), the host threads narrow the rows of a prefix of the
+ * vocabulary (half of it by default; the environment variable
+ * WMD_DROPIN_HOST_SHARE, 0 to 1, sets the share) to FP32 and copy them while
+ * the GPU reads, above the prefix, only the rows of the words that occur in
+ * the target matrix or in r, in FP64 directly from host memory.  Pageable
+ * embeddings are narrowed on the host whole (copied whole with a share of 0
+ * or fewer than 4 host threads).  Results are the same on every path.  No
+ * reference counterpart (a measurement aid). */
 uint64_t wmd_dropin_h2d_bytes(void);
 
 /* ---------------------------------------------------------------------------
