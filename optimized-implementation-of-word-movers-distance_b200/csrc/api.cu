@@ -1599,6 +1599,9 @@ wmd_status set_embeddings_split(wmd_handle* h, const double* vecs, const double*
   CK(h->need_count.ensure(sizeof(unsigned long long)));
   CK(h->rows32.ensure(std::max<size_t>(wh, 1) * d * sizeof(float)));
   if (wh > 0) {
+    // (a call that failed part-way may have left copies from the staging
+    // slots in flight: they end before the slots are written again)
+    if (h->stream2) CK(cudaStreamSynchronize(h->stream2));
     CK(h->hstage.ensure(kStageSlots * kStageSlotBytes(d)));
     if (!h->stream2) CK(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
     if (!h->ev_split) CK(cudaEventCreateWithFlags(&h->ev_split, cudaEventDisableTiming));
