@@ -74,6 +74,9 @@ namespace wmd {
 #ifndef WMD_SOLVE_UNROLL  // staged rounds in flight per step
 #define WMD_SOLVE_UNROLL 2
 #endif
+#ifndef WMD_SOLVE_SKIP_PAD  // documents shorter than the register rounds skip the rest
+#define WMD_SOLVE_SKIP_PAD 1
+#endif
 #ifndef WMD_SOLVE_DOT_CHAINS  // independent accumulators per dot product
 #define WMD_SOLVE_DOT_CHAINS 2
 #endif
@@ -506,12 +509,24 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
         float sreg[RR], oreg[RR];
 #pragma unroll
         for (int t = 0; t < RR; ++t) oreg[t] = vold_at(t * WPS + g);
+        if (WMD_SOLVE_SKIP_PAD && RR > 1 && rr < RR) {
+          // A document of fewer rounds than the register rounds: only the
+          // rounds it fills (the others hold padding rows, whose v = 0 adds
+          // exactly nothing to x).  Round 0 always runs: it starts x.
+          sreg[0] = dot(reg[0], u2);
+          axpy_first(reg[0], vweight(creg[0], sreg[0], g, oreg[0]), x2);
 #pragma unroll
-        for (int t = 0; t < RR; ++t) sreg[t] = dot(reg[t], u2);
-        axpy_first(reg[0], vweight(creg[0], sreg[0], g, oreg[0]), x2);
+          for (int t = 1; t < RR; ++t)
+            if (t < rr)
+              axpy(reg[t], vweight(creg[t], dot(reg[t], u2), t * WPS + g, oreg[t]), x2);
+        } else {
 #pragma unroll
-        for (int t = 1; t < RR; ++t)
-          axpy(reg[t], vweight(creg[t], sreg[t], t * WPS + g, oreg[t]), x2);
+          for (int t = 0; t < RR; ++t) sreg[t] = dot(reg[t], u2);
+          axpy_first(reg[0], vweight(creg[0], sreg[0], g, oreg[0]), x2);
+#pragma unroll
+          for (int t = 1; t < RR; ++t)
+            axpy(reg[t], vweight(creg[t], sreg[t], t * WPS + g, oreg[t]), x2);
+        }
       }
       constexpr int U = SolveCfg<LPW>::kUnroll;
       int t = 0;
