@@ -567,8 +567,11 @@ int warp_shape_for(wmd_handle* h, const float* K, int ld, float expo, uint32_t c
   while (k < 5 && (32u << k) < cap) ++k;
   if (h->warp_shape[k] != -2) return h->warp_shape[k];
   if (!h->autotune || !can_sync) return -1;
+  // The query's own update count (at most 15): the shapes rank differently
+  // for the per-launch part (row gathers, final half-step) and the
+  // per-update part, so a short tuning launch can pick the wrong one.
   SolveCtl c2 = ctl;
-  c2.max_iter = 4;
+  c2.max_iter = std::min(std::max(ctl.max_iter, 1), 15);
   c2.tol = 0.f;
   c2.iters = nullptr;
   c2.u0 = nullptr;
@@ -578,20 +581,37 @@ int warp_shape_for(wmd_handle* h, const float* K, int ld, float expo, uint32_t c
     if (a) cudaEventDestroy(a);
     return -1;
   }
+  // The candidates differ by a few percent of a launch, near the event
+  // clock's resolution for one launch: each is timed over kRuns groups of
+  // kPer launches, the groups of the candidates interleaved.
+  constexpr int kMaxShapes = 8, kRuns = 3, kPer = 2;
+  const int ns = std::min(solve_shape_count(), kMaxShapes);
+  float tot[kMaxShapes];
+  bool ok[kMaxShapes];
+  for (int sh = 0; sh < ns; ++sh) {
+    tot[sh] = 0.f;
+    ok[sh] = launch_solve(K, nullptr, ld, expo, cap, sel, t, c2, out, h->stream, sh) >= 0;
+  }
+  for (int run = 0; run < kRuns; ++run)
+    for (int sh = 0; sh < ns; ++sh) {
+      if (!ok[sh]) continue;
+      cudaEventRecord(a, h->stream);
+      for (int i = 0; i < kPer; ++i)
+        launch_solve(K, nullptr, ld, expo, cap, sel, t, c2, out, h->stream, sh);
+      cudaEventRecord(b, h->stream);
+      float ms = 0.f;
+      if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess)
+        tot[sh] += ms;
+      else
+        ok[sh] = false;
+    }
   float best = 1e30f;
   int bi = -1;
-  for (int sh = 0; sh < solve_shape_count(); ++sh) {
-    if (launch_solve(K, nullptr, ld, expo, cap, sel, t, c2, out, h->stream, sh) < 0) continue;
-    cudaEventRecord(a, h->stream);
-    launch_solve(K, nullptr, ld, expo, cap, sel, t, c2, out, h->stream, sh);
-    cudaEventRecord(b, h->stream);
-    float ms = 0.f;
-    if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess &&
-        ms < best) {
-      best = ms;
+  for (int sh = 0; sh < ns; ++sh)
+    if (ok[sh] && tot[sh] < best) {
+      best = tot[sh];
       bi = sh;
     }
-  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   h->warp_shape[k] = bi;

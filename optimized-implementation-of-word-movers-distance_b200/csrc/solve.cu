@@ -118,6 +118,13 @@ __device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
 #endif
 }
 
+// The hardware base-2 logarithm with subnormal inputs flushed to zero.
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 struct Row {  // one lane's 32-dimension slice of a K (or KM) row
   float4 c[8];
 };
@@ -645,24 +652,37 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
     // Final half-step (fused:339-393): WMD = sum_k v_k (KM_k . u), FP64 sum.
     const float km_scale = FROM_KM ? 1.f : 0.69314718f / expo;  // ln 2 / expo
     double acc = 0.0;
-    for (int t = 0; t < rounds; ++t) {
-      Row rk;
-      float ck;
-      const int k = t * WPS + g;
-      if (t < rr) {
-        rk = reg[0];
-        ck = creg[0];
+    // KM_k . u with KM_i = K_i M_i = K_i log2(K_i) ln2 / expo.  Outside the
+    // row-scaled panel every K entry is 0 (padding) or normal (lambda M stays
+    // below the scaling limit, K >= e^-80), so the flush-to-zero hardware
+    // logarithm of max(K, 2^-126) gives log2 K exactly as the subnormal-aware
+    // form and 0 x (-126) = 0 for the zeros; the row-scaled panel's subnormal
+    // entries (weighted by a large u) keep the subnormal-aware form.
+    auto km_dot = [&](const Row& rk, bool exact) -> float {
+      float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int i = 1; i < RR; ++i)
-          if (t == i) {
-            rk = reg[i];
-            ck = creg[i];
-          }
-      } else if (t < rr + sr) {
-        load_staged(t - rr, rk, ck);
-      } else {
-        load_global(Kd, k, rk, ck, true);
+      for (int c = 0; c < 8; ++c) {
+        const float4 kk = rk.c[c];
+        float l0, l1, l2, l3;
+        if (exact) {
+          l0 = kk.x > 0.f ? __log2f(kk.x) : 0.f;
+          l1 = kk.y > 0.f ? __log2f(kk.y) : 0.f;
+          l2 = kk.z > 0.f ? __log2f(kk.z) : 0.f;
+          l3 = kk.w > 0.f ? __log2f(kk.w) : 0.f;
+        } else {
+          l0 = lg2_ftz(fmaxf(kk.x, 0x1p-126f));
+          l1 = lg2_ftz(fmaxf(kk.y, 0x1p-126f));
+          l2 = lg2_ftz(fmaxf(kk.z, 0x1p-126f));
+          l3 = lg2_ftz(fmaxf(kk.w, 0x1p-126f));
+        }
+        const float2 uk0 = __fmul2_rn(u2[2 * c], make_float2(kk.x, kk.y));
+        const float2 uk1 = __fmul2_rn(u2[2 * c + 1], make_float2(kk.z, kk.w));
+        a = ffma2(uk0, make_float2(l0, l1), a);
+        a = ffma2(uk1, make_float2(l2, l3), a);
       }
+      return a.x + a.y;
+    };
+    auto final_word = [&](const Row& rk, float ck, int k) {
       const float v = weight(ck, dot(rk, u2));
       float tk;
       if (FROM_KM) {
@@ -671,21 +691,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
         load_global(KM, k, rm, cm, false);
         tk = dot(rm, u2);
       } else {
-        // KM_i = K_i M_i = K_i log2(K_i) ln2 / expo; K_i = 0 contributes 0.
-        float2 a = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const float4 kk = rk.c[c];
-          const float l0 = kk.x > 0.f ? __log2f(kk.x) : 0.f;
-          const float l1 = kk.y > 0.f ? __log2f(kk.y) : 0.f;
-          const float l2 = kk.z > 0.f ? __log2f(kk.z) : 0.f;
-          const float l3 = kk.w > 0.f ? __log2f(kk.w) : 0.f;
-          const float2 uk0 = make_float2(u2[2 * c].x * kk.x, u2[2 * c].y * kk.y);
-          const float2 uk1 = make_float2(u2[2 * c + 1].x * kk.z, u2[2 * c + 1].y * kk.w);
-          a = ffma2(uk0, make_float2(l0, l1), a);
-          a = ffma2(uk1, make_float2(l2, l3), a);
-        }
-        tk = a.x + a.y;
+        tk = MROW() ? km_dot(rk, true) : km_dot(rk, false);
 #pragma unroll
         for (int off = 1; off < LPW; off <<= 1)
           tk += __shfl_xor_sync(0xffffffffu, tk, off);
@@ -698,6 +704,19 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
           acc += (double)ck * (double)__ldg(&MROW()[id]);
         }
       }
+    };
+    // Register rounds by their fixed registers, then the staged and L2 ones.
+#pragma unroll
+    for (int t = 0; t < RR; ++t)
+      if (t < rr) final_word(reg[t], creg[t], t * WPS + g);
+    for (int t = rr; t < rounds; ++t) {
+      Row rk;
+      float ck;
+      if (t < rr + sr)
+        load_staged(t - rr, rk, ck);
+      else
+        load_global(Kd, t * WPS + g, rk, ck, true);
+      final_word(rk, ck, t * WPS + g);
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
