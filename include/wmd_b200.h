@@ -223,8 +223,9 @@ int wmd_last_batch_groups(wmd_handle* h);
  * layout (v_r <= 32, 64, 128, 256, 512, 1024): a candidate index (see
  * wmd_solve_shape_name), -1 for the build-time default, -2 not tuned yet.
  * Chosen on the first query of each layout after targets or embeddings are
- * set (each candidate timed on the real panel, 4 updates), unless tuning is
- * off (wmd_set_autotune).  No reference counterpart. */
+ * set (each candidate timed on the real panel at the query's update count,
+ * at most 15), unless tuning is off (wmd_set_autotune).  No reference
+ * counterpart. */
 wmd_status wmd_solve_shape_choices(wmd_handle* h, int* shapes);
 const char* wmd_solve_shape_name(int shape);
 

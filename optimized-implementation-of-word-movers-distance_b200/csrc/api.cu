@@ -557,7 +557,8 @@ int block_shape_for(wmd_handle* h, const void* K16, int ld16, float expo,
 // Launch shape of the plain warp solve for sources of up to `cap` words,
 // cached per lane layout; when not yet known and the call may synchronise,
 // each candidate (warps per CTA x CTAs per SM) is timed on the real panel and
-// target set (4 updates, CUDA events) and the fastest is kept.  -1: the
+// target set (the query's update count, at most 15; CUDA events) and the
+// fastest is kept.  -1: the
 // build-time default (tuning off, inside a capture, or not a plain solve).
 int warp_shape_for(wmd_handle* h, const float* K, int ld, float expo, uint32_t cap,
                    const SourceSel& sel, const Targets& t, const SolveCtl& ctl,
