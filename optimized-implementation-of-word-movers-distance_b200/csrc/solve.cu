@@ -682,7 +682,9 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
       }
       return a.x + a.y;
     };
-    auto final_word = [&](const Row& rk, float ck, int k) {
+    // exact: the row-scaled panel (its subnormal-aware logarithm and the
+    // + c_w m_w term).
+    auto final_word = [&](const Row& rk, float ck, int k, bool exact) {
       const float v = weight(ck, dot(rk, u2));
       float tk;
       if (FROM_KM) {
@@ -691,7 +693,7 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
         load_global(KM, k, rm, cm, false);
         tk = dot(rm, u2);
       } else {
-        tk = MROW() ? km_dot(rk, true) : km_dot(rk, false);
+        tk = km_dot(rk, exact);
 #pragma unroll
         for (int off = 1; off < LPW; off <<= 1)
           tk += __shfl_xor_sync(0xffffffffu, tk, off);
@@ -699,24 +701,48 @@ solve_kernel(const float* __restrict__ K, const float* __restrict__ KM, int ld_a
       }
       if (q == 0 && k < n) {
         acc += (double)v * (double)tk;
-        if (MROW()) {  // row-scaled panel: + c_w m_w (panel_rescale.cu)
+        if (exact) {  // row-scaled panel: + c_w m_w (panel_rescale.cu)
           const uint32_t id = k < ne ? sE[k].x : __ldg(&ent[b + k]).x;
           acc += (double)ck * (double)__ldg(&MROW()[id]);
         }
       }
     };
-    // Register rounds by their fixed registers, then the staged and L2 ones.
+    if (MROW()) {
+      // Row-scaled panel: one copy of the word body (the register rows
+      // selected per round), which keeps the final half-step's code small.
+      for (int t = 0; t < rounds; ++t) {
+        Row rk;
+        float ck;
+        if (t < rr) {
+          rk = reg[0];
+          ck = creg[0];
 #pragma unroll
-    for (int t = 0; t < RR; ++t)
-      if (t < rr) final_word(reg[t], creg[t], t * WPS + g);
-    for (int t = rr; t < rounds; ++t) {
-      Row rk;
-      float ck;
-      if (t < rr + sr)
-        load_staged(t - rr, rk, ck);
-      else
-        load_global(Kd, t * WPS + g, rk, ck, true);
-      final_word(rk, ck, t * WPS + g);
+          for (int i = 1; i < RR; ++i)
+            if (t == i) {
+              rk = reg[i];
+              ck = creg[i];
+            }
+        } else if (t < rr + sr) {
+          load_staged(t - rr, rk, ck);
+        } else {
+          load_global(Kd, t * WPS + g, rk, ck, true);
+        }
+        final_word(rk, ck, t * WPS + g, true);
+      }
+    } else {
+      // Register rounds by their fixed registers, then the staged and L2 ones.
+#pragma unroll
+      for (int t = 0; t < RR; ++t)
+        if (t < rr) final_word(reg[t], creg[t], t * WPS + g, false);
+      for (int t = rr; t < rounds; ++t) {
+        Row rk;
+        float ck;
+        if (t < rr + sr)
+          load_staged(t - rr, rk, ck);
+        else
+          load_global(Kd, t * WPS + g, rk, ck, true);
+        final_word(rk, ck, t * WPS + g, false);
+      }
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
